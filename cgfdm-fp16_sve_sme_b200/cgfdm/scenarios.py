@@ -1,0 +1,189 @@
+"""Synthetic model inputs in the reference's own file formats.
+
+The reference reads its run from ``params.json`` (src-new-FP32-SVE/
+getParams.cpp:55-242), ``station.json`` (station.cpp:83-187), a layered
+medium file (medium.cpp:98-130), a finite-fault source file
+(multiSource.cpp:14-87, 362-418) and, for real terrain, DEM tiles.  The
+public datasets behind those inputs are not available here, so the model
+shapes of the benchmark configurations are synthesised with seeded
+generators and written in exactly those formats:
+
+* terrain: an analytic Gaussian hill or a seeded Gaussian random field over
+  the padded grid (NX+6)x(NY+6), x fastest, heights in metres;
+* layered medium: ``int32 layers`` then per layer ``float32`` bottom depth
+  (km), Vs, Vp (km/s), rho (g/cc);
+* source: ``int32 npts, int32 nt, float32 dt`` then per point
+  ``float32 x, y, z, area, strike, dip, rake[nt], slip_rate[nt]``; x and y
+  are metres from the grid centre (the reader's map projection is the
+  identity on them), z is negative down.
+"""
+import json
+import math
+import os
+import struct
+
+import numpy as np
+
+HALO = 3
+
+DEFAULT_PARAMS = {
+    "TMAX": 1.0001, "DT": 0.008, "DH": 100.0, "NX": 64, "NY": 64, "NZ": 48,
+    "Depth(km)": 4.8, "centerX": 0, "centerY": 0, "IT_SKIP": 100000,
+    "sliceX": -1, "sliceY": -1, "sliceZ": -1, "sliceFreeSurf": 0,
+    "PX": 1, "PY": 1, "PZ": 1, "sourceX": 32, "sourceY": 32, "sourceZ": 24,
+    "centerLatitude": 0.0, "centerLongitude": 0.0,
+    "nPML": 12, "Non-Uniform": 0, "gauss_hill": 0, "useTerrain": 0, "useMedium": 0,
+    "useMultiSource": 0, "useSingleSource(ricker)": 1, "rickerfc": 1.5,
+    "ShenModel": 0, "Crust_1Medel": 0, "LayeredModel": 0, "LayeredFileName": "layers.bin",
+    "out": "output", "sourceDir": ".", "sourceFile": "source.bin", "SRTM90": 0,
+}
+
+
+def params(**over):
+    p = dict(DEFAULT_PARAMS)
+    p.update(over)
+    return p
+
+
+def nt_of(p):
+    """NT = (int)(TMAX / DT) with DT stored as double (propagate.cpp:35-36)."""
+    return int(p["TMAX"] / np.float32(p["DT"]))
+
+
+def grid_dims(p):
+    nx, ny, nz = p["NX"], p["NY"], p["NZ"]
+    d = {"nx": nx, "ny": ny, "nz": nz, "nx_": nx + 2 * HALO, "ny_": ny + 2 * HALO,
+         "nz_": nz + 2 * HALO}
+    d["num"] = d["nx_"] * d["ny_"] * d["nz_"]
+    return d
+
+
+def xy_axes(p):
+    """Global x, y coordinates of the padded grid (coord.cpp:137-138)."""
+    I = np.arange(p["NX"] + 2 * HALO)
+    J = np.arange(p["NY"] + 2 * HALO)
+    DH = np.float32(p["DH"])
+    x = (I - HALO) * DH - p["centerX"] * DH
+    y = (J - HALO) * DH - p["centerY"] * DH
+    return x.astype(np.float64), y.astype(np.float64)
+
+
+def gaussian_hill(p, amp, x0, y0, width):
+    """h = amp * exp(-((x-x0)^2 + (y-y0)^2) / width^2) on the padded grid."""
+    x, y = xy_axes(p)
+    X, Y = np.meshgrid(x, y)
+    return (amp * np.exp(-((X - x0) ** 2 + (Y - y0) ** 2) / width ** 2)).astype(np.float32)
+
+
+def random_terrain(p, rms, corr, seed):
+    """Seeded Gaussian random field with a Gaussian spectrum of correlation
+    length ``corr`` (m), rescaled to RMS height ``rms`` (m), made
+    non-negative-mean by shifting its minimum to zero."""
+    rng = np.random.default_rng(seed)
+    ny, nx = p["NY"] + 2 * HALO, p["NX"] + 2 * HALO
+    white = rng.standard_normal((ny, nx))
+    kx = np.fft.fftfreq(nx, d=p["DH"]) * 2 * np.pi
+    ky = np.fft.fftfreq(ny, d=p["DH"]) * 2 * np.pi
+    KX, KY = np.meshgrid(kx, ky)
+    filt = np.exp(-(KX ** 2 + KY ** 2) * corr ** 2 / 8.0)
+    field = np.real(np.fft.ifft2(np.fft.fft2(white) * filt))
+    field -= field.mean()
+    field *= rms / max(field.std(), 1e-12)
+    return field.astype(np.float32)
+
+
+def layered_bytes(layers):
+    """layers: [(bottom_depth_km, vs_kms, vp_kms, rho_gcc), ...]."""
+    out = struct.pack("<i", len(layers))
+    for row in layers:
+        out += struct.pack("<4f", *row)
+    return out
+
+
+def ricker_rate(t, f0, t0):
+    """Ricker wavelet (1 - 2 r^2) exp(-r^2), r = pi f0 (t - t0)."""
+    r = np.pi * f0 * (t - t0)
+    return (1.0 - 2.0 * r ** 2) * np.exp(-r ** 2)
+
+
+def gaussian_rate(t, width, t0):
+    """Unit-area Gaussian slip-rate function of standard deviation ``width``."""
+    return np.exp(-0.5 * ((t - t0) / width) ** 2) / (width * math.sqrt(2 * math.pi))
+
+
+def source_bytes(points, nt, dt):
+    """points: list of dicts x, y, z, area, strike, dip, rake[nt], rate[nt]."""
+    out = struct.pack("<iif", len(points), nt, dt)
+    for q in points:
+        out += struct.pack("<6f", q["x"], q["y"], q["z"], q["area"], q["strike"], q["dip"])
+        out += np.asarray(q["rake"], np.float32).tobytes()
+        out += np.asarray(q["rate"], np.float32).tobytes()
+    return out
+
+
+def double_couple_point(x, y, z, m0, mu, strike, dip, rake, nt, dt, stf):
+    """One double-couple point source through the finite-fault path: area is
+    M0/mu (unit slip), rate is the slip-rate time function ``stf`` sampled at
+    dt.  A zero-area anchor at z=0 keeps the reader's depth shift
+    (z - max z, multiSource.cpp:211-225) from moving the source."""
+    t = np.arange(nt) * dt
+    pts = [dict(x=x, y=y, z=z, area=m0 / mu, strike=strike, dip=dip,
+                rake=np.full(nt, rake, np.float32), rate=stf(t).astype(np.float32)),
+           dict(x=x, y=y, z=0.0, area=0.0, strike=strike, dip=dip,
+                rake=np.full(nt, rake, np.float32), rate=np.zeros(nt, np.float32))]
+    return source_bytes(pts, nt, dt)
+
+
+def finite_fault(cx, cy, cz, length, width, nl, nw, strike, dip, rake, mean_slip,
+                 vs_rupture, stf_width, nt, dt, seed, mu=3.2e10, surface_z=0.0):
+    """Planar fault of nl x nw point sources centred at (cx, cy, cz) with
+    seeded log-normal slip of mean ``mean_slip``; rupture starts at the
+    centre and spreads at ``vs_rupture``; each point's slip rate is a Gaussian
+    of width ``stf_width`` (s) delayed by its rupture time, scaled by its
+    slip.  Returns the source file bytes."""
+    rng = np.random.default_rng(seed)
+    sigma = 0.5
+    slip = rng.lognormal(mean=math.log(mean_slip) - sigma ** 2 / 2, sigma=sigma, size=(nw, nl))
+    s, d = math.radians(strike), math.radians(dip)
+    us = np.array([math.sin(s), math.cos(s), 0.0])             # along strike
+    ud = np.array([math.cos(d) * math.cos(s), -math.cos(d) * math.sin(s),
+                   -math.sin(d)])                               # down dip
+    t = np.arange(nt) * dt
+    area = (length / nl) * (width / nw)
+    pts = []
+    for iw in range(nw):
+        for il in range(nl):
+            a = (il + 0.5) / nl * length - length / 2
+            b = (iw + 0.5) / nw * width - width / 2
+            pos = np.array([cx, cy, cz]) + a * us + b * ud
+            delay = math.hypot(a, b) / vs_rupture
+            rate = slip[iw, il] * gaussian_rate(t, stf_width, delay + 3 * stf_width)
+            pts.append(dict(x=pos[0], y=pos[1], z=pos[2], area=area, strike=strike, dip=dip,
+                            rake=np.full(nt, rake, np.float32), rate=rate.astype(np.float32)))
+    pts.append(dict(x=cx, y=cy, z=surface_z, area=0.0, strike=strike, dip=dip,
+                    rake=np.full(nt, rake, np.float32), rate=np.zeros(nt, np.float32)))
+    return source_bytes(pts, nt, dt)
+
+
+def write_run_dir(dirpath, p, stations=None, terrain=None, layers=None, source=None):
+    """Writes params.json, station.json, terrain_input.bin, the layered file
+    and the source file of a run into ``dirpath``."""
+    os.makedirs(dirpath, exist_ok=True)
+    with open(os.path.join(dirpath, "params.json"), "w") as f:
+        json.dump(p, f, indent=1)
+    if stations is not None:
+        with open(os.path.join(dirpath, "station.json"), "w") as f:
+            json.dump({"station(point)": stations}, f, indent=1)
+    if terrain is not None:
+        np.asarray(terrain, np.float32).tofile(os.path.join(dirpath, "terrain_input.bin"))
+    if layers is not None:
+        with open(os.path.join(dirpath, p["LayeredFileName"]), "wb") as f:
+            f.write(_as_bytes(layers))
+    if source is not None:
+        os.makedirs(os.path.join(dirpath, p["sourceDir"]), exist_ok=True)
+        with open(os.path.join(dirpath, p["sourceDir"], p["sourceFile"]), "wb") as f:
+            f.write(_as_bytes(source))
+
+
+def _as_bytes(x):
+    return x.tobytes() if isinstance(x, np.ndarray) else bytes(x)

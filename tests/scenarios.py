@@ -1,0 +1,147 @@
+"""Small test configurations shared by the golden generator and the tests.
+
+Each scenario is a dict with ``params`` (params.json content), ``stations``
+(station.json content), and optionally ``terrain`` (float32 array of the
+padded (NY+6, NX+6) grid), ``layers`` (layered-model file bytes as uint8)
+and ``source`` (finite-fault file bytes as uint8).
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(REPO, "cgfdm-fp16_sve_sme_b200")
+if PKG not in sys.path:
+    sys.path.insert(0, PKG)
+from cgfdm import scenarios as S  # noqa: E402
+
+HALO = 3
+# (irk, (FB1, FB2, FB3)) of the stage fixtures: every RK stage, mixed sign
+# triples from the MacCormack schedule (propagate.cpp:107-117).
+STAGE_CASES = [(0, (-1, -1, -1)), (1, (1, 1, 1)), (2, (-1, 1, -1)), (3, (1, -1, 1))]
+
+TWO_LAYERS = [(0.5, 2.0, 3.5, 2.2), (1000.0, 3.464, 6.0, 2.67)]
+THREE_LAYERS = [(0.6, 2.6, 4.5, 2.3), (1.2, 3.35, 5.8, 2.6), (1000.0, 3.75, 6.5, 2.8)]
+
+
+def as_u8(b):
+    return np.frombuffer(bytes(b), dtype=np.uint8).copy()
+
+
+def grid_dims(p):
+    return S.grid_dims(p)
+
+
+def stage_small():
+    """12 x 10 x 10 curvilinear grid: Gaussian-hill terrain, two layers,
+    3-cell PML (bottom, four sides) and the free surface on top."""
+    p = S.params(NX=12, NY=10, NZ=10, nPML=3, DH=100.0, DT=0.008, TMAX=0.0161,
+                 **{"Depth(km)": 1.0}, centerX=6, centerY=5, useTerrain=1, useMedium=1,
+                 LayeredModel=1, sourceX=6, sourceY=5, sourceZ=5, out="out")
+    terrain = S.gaussian_hill(p, amp=300.0, x0=100.0, y0=-50.0, width=400.0)
+    return {"params": p, "stations": {}, "terrain": terrain,
+            "layers": as_u8(S.layered_bytes(TWO_LAYERS))}
+
+
+def run_point():
+    """Flat half-space, homogeneous medium, smoothed explosive point source
+    (the single-source path), 24 x 20 x 16 grid, 40 steps."""
+    p = S.params(NX=24, NY=20, NZ=16, nPML=4, DH=100.0, DT=0.008, TMAX=0.3201,
+                 centerX=12, centerY=10, IT_SKIP=13, sliceFreeSurf=1,
+                 sourceX=11, sourceY=9, sourceZ=8, rickerfc=6.0, out="out")
+    stations = {"A": [5, 5, 15], "B": [11, 9, 15], "C": [18, 14, 15], "D": [11, 9, 12],
+                "E": [4, 16, 10]}
+    return {"params": p, "stations": stations}
+
+
+def run_fault():
+    """Gaussian-hill terrain, layered medium, finite-fault source through
+    the multi-source path, 24 x 22 x 18 grid, 40 steps."""
+    p = S.params(NX=24, NY=22, NZ=18, nPML=4, DH=100.0, DT=0.006, TMAX=0.2401,
+                 **{"Depth(km)": 1.6}, centerX=12, centerY=11, IT_SKIP=13,
+                 sliceFreeSurf=1, useTerrain=1, useMedium=1, LayeredModel=1,
+                 useMultiSource=1, **{"useSingleSource(ricker)": 0}, out="out")
+    terrain = S.gaussian_hill(p, amp=250.0, x0=-200.0, y0=100.0, width=600.0)
+    nt = 60
+    src = S.finite_fault(cx=0.0, cy=0.0, cz=-700.0, length=600.0, width=300.0, nl=4, nw=2,
+                         strike=90.0, dip=30.0, rake=60.0, mean_slip=1.5, vs_rupture=2400.0,
+                         stf_width=0.02, nt=nt, dt=0.006, seed=7)
+    stations = {"A": [5, 5, 17], "B": [12, 11, 17], "C": [19, 16, 17], "D": [12, 11, 12],
+                "E": [6, 17, 9]}
+    return {"params": p, "stations": stations, "terrain": terrain,
+            "layers": as_u8(S.layered_bytes(TWO_LAYERS)), "source": as_u8(src)}
+
+
+def write_inputs(sc, dirpath):
+    S.write_run_dir(dirpath, sc["params"], stations=sc.get("stations") or {},
+                    terrain=sc.get("terrain"), layers=sc.get("layers"),
+                    source=sc.get("source"))
+
+
+def read_outputs(sc, outdir):
+    """Reads the reference's single-rank outputs (station.cpp:382-405,
+    PGV.cpp:103-111, data_io.cpp:323-495)."""
+    p = sc["params"]
+    g = grid_dims(p)
+    nt = S.nt_of(p)
+    res = {}
+    fn = os.path.join(outdir, "station_mpi_0_0_0.bin")
+    if os.path.exists(fn):
+        raw = np.fromfile(fn, dtype=np.uint8)
+        nsta = len(sc["stations"])
+        res["station_xyz"] = raw[: 12 * nsta].view(np.int32).reshape(nsta, 3)
+        res["station_wave"] = raw[12 * nsta:].view(np.float32).reshape(nsta, nt, 9)
+    fn = os.path.join(outdir, "PGV_Z_mpi_0_0_0.bin")
+    if os.path.exists(fn):
+        res["pgv"] = np.fromfile(fn, np.float32).reshape(g["ny"], g["nx"], 2)
+    snaps = []
+    for it in range(0, nt, p["IT_SKIP"]):
+        fn = os.path.join(outdir, "FreeSurfVz_%d_Z_mpi_0_0_0.bin" % it)
+        if os.path.exists(fn):
+            v = [np.fromfile(os.path.join(outdir, "FreeSurfV%s_%d_Z_mpi_0_0_0.bin" % (c, it)),
+                             np.float32).reshape(g["ny"], g["nx"]) for c in "xyz"]
+            snaps.append(np.stack(v))
+    if snaps:
+        res["freesurf"] = np.stack(snaps)
+        res["freesurf_its"] = np.arange(0, nt, p["IT_SKIP"])[: len(snaps)]
+    return res
+
+
+def slab_points(p):
+    nx, ny, nz, n = p["NX"], p["NY"], p["NZ"], p["nPML"]
+    return [n * ny * nz, nx * n * nz, nx * ny * n, n * ny * nz, nx * n * nz]
+
+
+def random_state(p, seed):
+    """Seeded input state of one stage: wavefield W, RK accumulators t and m
+    (each 9 x num, zero in the halo like the reference's, velocities ~1e-2,
+    stresses ~1e5) and the PML auxiliaries (5 slabs x [Aux, t, m])."""
+    rng = np.random.default_rng(seed)
+    g = grid_dims(p)
+    scale = np.array([1e-2] * 3 + [1e5] * 6, np.float32)[:, None, None, None]
+
+    def wave():
+        w = np.zeros((9, g["nz_"], g["ny_"], g["nx_"]), np.float32)
+        inner = rng.standard_normal((9, g["nz"], g["ny"], g["nx"])).astype(np.float32)
+        w[:, HALO:-HALO, HALO:-HALO, HALO:-HALO] = inner * scale
+        return w.reshape(-1)
+
+    st = {"W": wave(), "t": wave(), "m": wave()}
+    aux = []
+    sc = np.array([1e-2] * 3 + [1e5] * 6, np.float32)
+    for n in slab_points(p):
+        for _ in range(3):
+            aux.append((rng.standard_normal((n, 9)).astype(np.float32) * sc).reshape(-1))
+    st["aux"] = np.concatenate(aux)
+    return st
+
+
+def load_golden(name):
+    d = np.load(os.path.join(REPO, "tests", "golden", name))
+    out = {k: d[k] for k in d.files}
+    out["params"] = json.loads(str(out.pop("params_json")))
+    if "stations_json" in out:
+        out["stations"] = json.loads(str(out.pop("stations_json")))
+    return out
