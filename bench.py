@@ -1,0 +1,430 @@
+"""Benchmark of the CGFDM hot path on B200 (one JSON line on stdout).
+
+A step is one full RK4 time step (sources, four fused stages, stations, PGV)
+over the whole grid of the workload.  Metric: grid-point updates per second
+per RK4 step (Gpt-updates/s).  Multi-GPU: independent replicas (the path is
+not sharded), weak scaling, max time over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2]
+                  [--precision fp32] [--impl ours|reference]
+
+--impl reference times the reference's own scalar CPU build (oracle/_ref,
+compiled in place from the reference sources, run on all host cores as MPI
+ranks through the shared-memory MPI shim) on the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "cgfdm-fp16_sve_sme_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+from cgfdm import scenarios as S  # noqa: E402
+
+REF_EXE = os.path.join(ROOT, "oracle", "_ref", "cgfdm_ref_fp32")
+METRIC = "Gpt-updates/s per RK4 step"
+UNIT = "Gpt-updates/s"
+# Algorithmic HBM bytes per grid point per RK4 step of the fused stage kernels
+# in FP32: per stage 9 stage-input + 12 coefficient reads and 9 output
+# writes; W_n reads in stages 1-2; the RK accumulator written in stage 0,
+# read+written in stages 1-2, read in stage 3 (4 bytes each).
+BYTES_PER_POINT_STEP = {"fp32": 768, "fp64": 1536, "fp16": 384, "bf16": 384}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# --------------------------------------------------------------------------
+# workloads (synthetic inputs with the shapes of the benchmark configurations)
+# --------------------------------------------------------------------------
+C2_LAYERS = [(2.0, 2.6, 4.5, 2.3), (8.0, 3.35, 5.8, 2.6), (1000.0, 3.75, 6.5, 2.8)]
+
+
+def workload_c2(nsteps_total):
+    """401 x 401 x 201 Gaussian hill (1500 m at x = y = 20 km, 5 km width),
+    bottom at -20 km, three layers, 20-cell PML, explosive Ricker source
+    (f0 = 2 Hz) 3 km under the hill flank, 121 surface stations."""
+    NX, NY, NZ, DH = 401, 401, 201, 100.0
+    dt = 0.008
+    p = S.params(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=dt, TMAX=(nsteps_total + 0.5) * dt,
+                 **{"Depth(km)": 20.0}, centerX=0, centerY=0, nPML=20, useTerrain=1,
+                 useMedium=1, LayeredModel=1, rickerfc=2.0, IT_SKIP=10 ** 7, out="out")
+    terrain = S.gaussian_hill(p, amp=1500.0, x0=20000.0, y0=20000.0, width=5000.0)
+    # source at i=170, j=200, 3 km below the local surface
+    h = float(terrain[200 + 3, 170 + 3])
+    dz = (h + 20000.0) / (NZ - 1)
+    p.update(sourceX=170, sourceY=200, sourceZ=int(round(NZ - 1 - 3000.0 / dz)))
+    stations = {"S%03d" % (a * 11 + b): [50 + 30 * a, 50 + 30 * b, NZ - 1]
+                for a in range(11) for b in range(11)}
+    return {"name": "c2-gaussian-hill-401x401x201", "params": p, "stations": stations,
+            "terrain": terrain, "layers": S.layered_bytes(C2_LAYERS)}
+
+
+def workload_c3(n, nsteps_total):
+    """n x n x 401 PerformanceTest shape: seeded random terrain (500 m RMS,
+    10 km correlation), the C2 layers with a seeded +-5 % velocity
+    perturbation, an 80 x 40 point finite fault (40 x 20 km, strike 90,
+    dip 30, log-normal slip of mean 1.5 m, rupture at 0.8 Vs, Gaussian STF of
+    1 s)."""
+    NZ, DH, dt = 401, 100.0, 0.008
+    p = S.params(NX=n, NY=n, NZ=NZ, DH=DH, DT=dt, TMAX=(nsteps_total + 0.5) * dt,
+                 **{"Depth(km)": 40.0}, centerX=n // 2, centerY=n // 2, nPML=12,
+                 useTerrain=1, useMedium=1, LayeredModel=1, useMultiSource=1,
+                 **{"useSingleSource(ricker)": 0}, IT_SKIP=10 ** 7, out="out",
+                 mediumPerturbation=0.05, mediumSeed=3)
+    terrain = S.random_terrain(p, rms=500.0, corr=10000.0, seed=11)
+    fault_len = min(40000.0, (n - 40) * DH * 0.6)
+    fault_wid = fault_len / 2
+    nt_src = nsteps_total + 8
+    src = S.finite_fault(cx=0.0, cy=0.0, cz=-12000.0, length=fault_len, width=fault_wid,
+                         nl=80, nw=40, strike=90.0, dip=30.0, rake=90.0, mean_slip=1.5,
+                         vs_rupture=0.8 * 3350.0, stf_width=1.0, nt=nt_src, dt=dt, seed=5,
+                         surface_z=float(terrain.max()))
+    stations = {"S%03d" % (a * 11 + b): [n // 12 * (a + 1), n // 12 * (b + 1), NZ - 1]
+                for a in range(11) for b in range(11)}
+    return {"name": "c3-perftest-%dx%dx401" % (n, n), "params": p, "stations": stations,
+            "terrain": terrain, "layers": S.layered_bytes(C2_LAYERS), "source": src}
+
+
+def make_workload(name, nsteps_total):
+    if name == "c2":
+        return workload_c2(nsteps_total)
+    m = re.fullmatch(r"c3-(\d+)", name)
+    if m:
+        return workload_c3(int(m.group(1)), nsteps_total)
+    raise SystemExit("unknown workload " + name)
+
+
+def write_workload(w, d):
+    S.write_run_dir(d, w["params"], stations=w["stations"], terrain=w.get("terrain"),
+                    layers=w.get("layers"), source=w.get("source"))
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+# --------------------------------------------------------------------------
+# reference arm / CPU baseline: the reference's own CPU build, all host cores
+# --------------------------------------------------------------------------
+def pick_decomposition(p, cores):
+    """PX*PY*PZ <= cores with every rank at least max(nPML, 8) cells per axis
+    (init_grid.cpp:109-117), preferring the largest rank count."""
+    best = (1, 1, 1)
+    lim = max(p["nPML"], 8)
+    for px in range(1, cores + 1):
+        if p["NX"] // px < lim:
+            break
+        for py in range(1, cores // px + 1):
+            if p["NY"] // py < lim:
+                break
+            for pz in range(1, cores // (px * py) + 1):
+                if p["NZ"] // pz < lim:
+                    break
+                if px * py * pz > best[0] * best[1] * best[2]:
+                    best = (px, py, pz)
+    return best
+
+
+def run_reference(w, nsteps, cores, timeout_s=900):
+    """Runs the reference on a copy of the workload for nsteps steps with
+    MPI ranks = cores; returns (seconds per step over the timed 10-step
+    blocks after the first, ranks used, steps timed)."""
+    if not os.path.exists(REF_EXE):
+        raise RuntimeError("reference build missing at %s (make -C oracle ref)" % REF_EXE)
+    p = dict(w["params"])
+    dt = np.float32(p["DT"])
+    total = 10 * max(2, math.ceil(nsteps / 10)) + 1
+    p["TMAX"] = float((total + 0.5) * dt)
+    px, py, pz = pick_decomposition(p, cores)
+    p.update(PX=px, PY=py, PZ=pz)
+    d = tempfile.mkdtemp(prefix="cgfdm_ref_")
+    try:
+        ww = dict(w)
+        ww["params"] = p
+        write_workload(ww, d)
+        env = dict(os.environ, CGFDM_SHIM_NPROC=str(px * py * pz), CGFDM_SHIM_TIMEOUT="600")
+        r = subprocess.run([REF_EXE], cwd=d, env=env, capture_output=True, text=True,
+                           timeout=timeout_s, start_new_session=True)
+        if r.returncode != 0:
+            raise RuntimeError("reference run failed (%d): %s" % (r.returncode, r.stdout[-400:] +
+                                                                  r.stderr[-400:]))
+        times = [float(m.group(1)) for m in
+                 re.finditer(r"Step time loss:\s*([0-9.eE+-]+)s", r.stdout)]
+        blocks = times[1:]  # it = 0 is the first step alone; later lines cover 10 steps
+        if len(blocks) > 1:
+            blocks = blocks[1:]  # first 10-step block is warm-up
+        if not blocks:
+            raise RuntimeError("no timing lines in the reference output")
+        return sum(blocks) / (10.0 * len(blocks)), px * py * pz, 10 * len(blocks)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+# --------------------------------------------------------------------------
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16", "bf16", "fp64"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "exact", "stream"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-baseline-steps", type=int, default=20)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    ws, rank, local = dist_env()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        w = make_workload(args.workload, args.warmup + args.steps + 2)
+        cores = os.cpu_count() or 1
+        try:
+            sps, ranks, timed = run_reference(w, args.warmup + args.steps, cores)
+        except Exception as e:  # noqa: BLE001
+            print(json.dumps({"impl": "reference", "unavailable": str(e)[:300]}))
+            return 0
+        npts = w["params"]["NX"] * w["params"]["NY"] * w["params"]["NZ"]
+        v = npts / sps / 1e9
+        sample = "%s, %d timed steps (10-step blocks after a warm-up block), %d MPI ranks" % (
+            w["name"], timed, ranks)
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
+            "steps": timed, "warmup": args.warmup, "ms_per_step": sps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w["name"], "precision": "fp32", "points": npts},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": ranks, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return 0
+
+    import torch
+    import cgfdm
+
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    prec = {"fp32": cgfdm.FP32, "fp16": cgfdm.FP16, "bf16": cgfdm.BF16, "fp64": cgfdm.FP64}[
+        args.precision]
+    kern = {"auto": cgfdm.KERNEL_AUTO, "exact": cgfdm.KERNEL_EXACT,
+            "stream": cgfdm.KERNEL_STREAM}[args.kernel]
+
+    total_steps = args.warmup + args.steps
+    w = make_workload(args.workload, max(total_steps, args.e2e_steps) + 2)
+    d = tempfile.mkdtemp(prefix="cgfdm_bench_")
+    write_workload(w, d)
+    t0 = time.perf_counter()
+    setup = cgfdm.setup_from_directory(d)
+    log("host setup %.1f s" % (time.perf_counter() - t0))
+    shutil.rmtree(d, ignore_errors=True)
+    desc0 = setup["desc"]
+    npts = desc0.nx * desc0.ny * desc0.nz
+    cjm = setup["cjm"]
+    if prec in (cgfdm.FP16, cgfdm.BF16):
+        # the scaled form needs the scaled coefficients of the FP16 setup
+        d2 = tempfile.mkdtemp(prefix="cgfdm_bench_")
+        write_workload(w, d2)
+        raise SystemExit("reduced-precision bench needs the scaled setup (not wired yet)")
+
+    def new_sim(nt):
+        desc = cgfdm.make_desc(desc0.nx, desc0.ny, desc0.nz, desc0.npml, desc0.dh, desc0.dt, nt,
+                               prec, kern, local)
+        sim = cgfdm.Simulation(desc)
+        sim.set_model(cjm, setup["rdz"])
+        if setup["point"] is not None:
+            sim.set_point_source(*setup["point"], setup["rickerfc"])
+        if setup["src_index"].size:
+            sim.set_fault_source(setup["src_index"], setup["moment_rate"], setup["src_nt"],
+                                 setup["src_dt"], scaled=True)
+        sim.set_stations(setup["stations"])
+        return sim
+
+    sim = new_sim(total_steps)
+    sim.set_timing(True)
+    stream = torch.cuda.current_stream()
+    sim.run(args.warmup, stream.cuda_stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        sim.run(args.steps, stream.cuda_stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    tm = sim.timing_ms()
+    stage_ms, stage_n = float(tm[1]), int(tm[2])
+    sim.close()
+    ms_t = torch.tensor([ms], device="cuda")
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = ws * npts * args.steps / (ms_max / 1e3) / 1e9
+
+    # end to end through the drop-in with host buffers (propagate())
+    e2e_steps = args.e2e_steps
+    desc = cgfdm.make_desc(desc0.nx, desc0.ny, desc0.nz, desc0.npml, desc0.dh, desc0.dt,
+                           e2e_steps, prec, kern, local)
+    sta = setup["stations"]
+    t0 = time.perf_counter()
+    out_sta, out_pgv, out_fs = cgfdm.propagate(
+        desc, cjm, setup["rdz"], point=setup["point"], rickerfc=setup["rickerfc"],
+        src_index=setup["src_index"] if setup["src_index"].size else None,
+        moment_rate=setup["moment_rate"] if setup["src_index"].size else None,
+        src_nt=setup["src_nt"], src_dt=setup["src_dt"], stations=sta)
+    e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], device="cuda")
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = ws * npts * e2e_steps / float(e2e_t.item()) / 1e9
+    h2d = cjm.nbytes + setup["rdz"].nbytes + setup["moment_rate"].nbytes + \
+        setup["src_index"].nbytes + sta.nbytes
+    d2h = out_sta.nbytes + out_pgv.nbytes + out_fs.nbytes
+
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    bpp = BYTES_PER_POINT_STEP[args.precision]
+    achieved = npts * bpp / 4.0 * stage_n / (stage_ms / 1e3) / 1e9 if stage_ms > 0 else None
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "stage_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get(args.workload, {}).get(args.precision)
+        except Exception:  # noqa: BLE001
+            traffic = None
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            sps, ranks, timed = run_reference(w, args.cpu_baseline_steps, os.cpu_count() or 1)
+            cpu = {"value": npts / sps / 1e9, "unit": UNIT, "cores": ranks, "kind": "reference",
+                   "sample": "%s, %d timed steps on %d MPI ranks (reference FP32 CPU build)" % (
+                       w["name"], timed, ranks)}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                   "sample": "unavailable: %s" % str(e)[:200]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp32": "f32", "fp64": "f64", "fp16": "f16-storage/f32",
+                      "bf16": "bf16-storage/f32"}[args.precision],
+            "data": "synthetic",
+            "config": {"workload": w["name"], "precision": args.precision,
+                       "grid": [desc0.nx, desc0.ny, desc0.nz], "points": npts,
+                       "kernel": args.kernel, "parallelism": "replicas" if ws > 1 else "single",
+                       "l2": "inputs larger than L2 (%.2f GB per wavefield buffer), no flush" % (
+                           9 * (desc0.nx + 6) * (desc0.ny + 6) * (desc0.nz + 6) * 4 / 1e9)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None, "traffic": traffic,
+                         "peak_source": peak_src, "bytes_per_point_step": bpp,
+                         "stage_ms_avg": stage_ms / max(stage_n, 1)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
+                    "d2h_bytes_per_step": d2h / e2e_steps, "steps": e2e_steps,
+                    "seconds": float(e2e_t.item())},
+            "gpu_launches": args.steps * (4 + 1 + 1),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

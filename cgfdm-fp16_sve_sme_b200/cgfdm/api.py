@@ -1,0 +1,202 @@
+"""Python host API over the C ABI (numpy arrays in, numpy arrays out).
+
+Mirrors the reference's hot-path interface: ``Simulation`` is the state that
+propagate() (src-new-FP32-SVE/propagate.cpp:24-228) owns on one rank,
+``propagate`` is the one-call drop-in, ``setup_from_directory`` is the host
+setup of run.cpp:56-131 and ``run_directory`` the whole program.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import CgfdmError, Desc, check, lib
+
+HALO = 3
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, np.float32)
+
+
+def make_desc(nx, ny, nz, npml, dh, dt, nt, precision=_lib.FP32, kernel=_lib.KERNEL_AUTO,
+              device=0):
+    return Desc(nx, ny, nz, npml, np.float32(dh), np.float32(dt), nt, precision, kernel, device)
+
+
+def device_bytes(desc):
+    n = C.c_int64()
+    check(lib().cgfdm_device_bytes(C.byref(desc), C.byref(n)))
+    return n.value
+
+
+class Simulation:
+    """One simulation resident on one GPU (a C-ABI handle)."""
+
+    def __init__(self, desc):
+        self.desc = desc
+        self.nx_, self.ny_, self.nz_ = desc.nx + 2 * HALO, desc.ny + 2 * HALO, desc.nz + 2 * HALO
+        self.num = self.nx_ * self.ny_ * self.nz_
+        self.nsurf = self.nx_ * self.ny_
+        h = C.c_void_p()
+        check(lib().cgfdm_create(C.byref(desc), C.byref(h)))
+        self._h = h
+        self.nsta = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cgfdm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- inputs -----------------------------------------------------------
+    def set_model(self, cjm, rdz):
+        cjm, rdz = _f32(cjm), _f32(rdz)
+        assert cjm.size == 13 * self.num and rdz.size == 18 * self.nsurf
+        check(lib().cgfdm_set_model(self._h, _ptr(cjm), _ptr(rdz)))
+
+    def set_point_source(self, sx, sy, sz, rickerfc):
+        check(lib().cgfdm_set_point_source(self._h, sx, sy, sz, np.float32(rickerfc)))
+
+    def set_fault_source(self, src_index, moment_rate, nt, dt, scaled=True):
+        idx = np.ascontiguousarray(src_index, np.int64)
+        mr = _f32(moment_rate)
+        assert mr.size == idx.size * nt * 6
+        check(lib().cgfdm_set_fault_source(self._h, _ptr(idx), _ptr(mr), idx.size, nt,
+                                           np.float32(dt), int(scaled)))
+
+    def set_stations(self, xyz):
+        xyz = np.ascontiguousarray(xyz, np.int32).reshape(-1, 3)
+        check(lib().cgfdm_set_stations(self._h, _ptr(xyz), len(xyz)))
+        self.nsta = len(xyz)
+
+    # ---- execution --------------------------------------------------------
+    def run(self, nsteps, stream=None):
+        check(lib().cgfdm_run(self._h, nsteps, stream))
+
+    def stage(self, irk, fb, stream=None):
+        check(lib().cgfdm_stage(self._h, irk, fb[0], fb[1], fb[2], stream))
+
+    def synchronize(self):
+        check(lib().cgfdm_synchronize(self._h))
+
+    def steps_done(self):
+        it = C.c_int32()
+        check(lib().cgfdm_steps_done(self._h, C.byref(it)))
+        return it.value
+
+    def set_timing(self, on=True):
+        check(lib().cgfdm_set_timing(self._h, int(on)))
+
+    def timing_ms(self):
+        ms = np.zeros(3, np.float32)
+        check(lib().cgfdm_get_timing(self._h, _ptr(ms)))
+        return ms
+
+    # ---- outputs ----------------------------------------------------------
+    def stations(self):
+        out = np.zeros((self.nsta, self.desc.nt, 9), np.float32)
+        if self.nsta:
+            check(lib().cgfdm_get_stations(self._h, _ptr(out)))
+        return out
+
+    def pgv(self):
+        out = np.zeros((self.desc.ny, self.desc.nx, 2), np.float32)
+        check(lib().cgfdm_get_pgv(self._h, _ptr(out)))
+        return out
+
+    def wavefield(self):
+        out = np.zeros(9 * self.num, np.float32)
+        check(lib().cgfdm_get_wavefield(self._h, _ptr(out)))
+        return out
+
+    def free_surface(self):
+        out = np.zeros((3, self.desc.ny, self.desc.nx), np.float32)
+        check(lib().cgfdm_get_free_surface(self._h, _ptr(out)))
+        return out
+
+    def aux_floats(self):
+        n = C.c_int64()
+        check(lib().cgfdm_aux_floats(self._h, C.byref(n)))
+        return n.value
+
+    def set_state(self, irk, W=None, t=None, m=None, aux=None):
+        W, t, m, aux = _f32(W), _f32(t), _f32(m), _f32(aux)
+        check(lib().cgfdm_set_state(self._h, irk, _ptr(W), _ptr(t), _ptr(m), _ptr(aux)))
+
+    def get_state(self):
+        W = np.zeros(9 * self.num, np.float32)
+        t = np.zeros_like(W)
+        m = np.zeros_like(W)
+        aux = np.zeros(3 * self.aux_floats(), np.float32)
+        check(lib().cgfdm_get_state(self._h, _ptr(W), _ptr(t), _ptr(m), _ptr(aux)))
+        return {"W": W, "t": t, "m": m, "aux": aux}
+
+
+def propagate(desc, cjm, rdz, *, point=None, rickerfc=0.0, src_index=None, moment_rate=None,
+              src_nt=0, src_dt=0.0, stations=None):
+    """propagate() drop-in with host buffers; returns (stations, pgv, free_surface)."""
+    cjm, rdz = _f32(cjm), _f32(rdz)
+    pxyz = None if point is None else np.ascontiguousarray(point, np.int32)
+    idx = None if src_index is None else np.ascontiguousarray(src_index, np.int64)
+    mr = _f32(moment_rate)
+    sta = None if stations is None else np.ascontiguousarray(stations, np.int32).reshape(-1, 3)
+    nsta = 0 if sta is None else len(sta)
+    out_sta = np.zeros((nsta, desc.nt, 9), np.float32)
+    out_pgv = np.zeros((desc.ny, desc.nx, 2), np.float32)
+    out_fs = np.zeros((3, desc.ny, desc.nx), np.float32)
+    check(lib().cgfdm_propagate(C.byref(desc), _ptr(cjm), _ptr(rdz), int(point is not None),
+                                _ptr(pxyz), np.float32(rickerfc), _ptr(idx), _ptr(mr),
+                                0 if idx is None else idx.size, src_nt, np.float32(src_dt),
+                                _ptr(sta), nsta, _ptr(out_sta) if nsta else None,
+                                _ptr(out_pgv), _ptr(out_fs)))
+    return out_sta, out_pgv, out_fs
+
+
+def setup_from_directory(run_dir):
+    """Host setup (params.json, station.json, model files) -> dict of arrays."""
+    s = _lib.Setup()
+    check(lib().cgfdm_setup_from_directory(run_dir.encode(), C.byref(s)))
+    try:
+        d = s.desc
+        nx_, ny_, nz_ = d.nx + 6, d.ny + 6, d.nz + 6
+        num, nsurf = nx_ * ny_ * nz_, nx_ * ny_
+        cp = lambda p, n: np.ctypeslib.as_array(p, shape=(n,)).copy() if n else np.zeros(0)
+        out = {
+            "desc": Desc(*[getattr(d, f) for f, _ in Desc._fields_]),
+            "cjm": cp(s.cjm, 13 * num), "rdz": cp(s.rdz, 18 * nsurf),
+            "coord": cp(s.coord, 3 * num), "medium": cp(s.medium, 3 * num),
+            "pml": cp(s.pml, 3 * (nx_ + ny_ + nz_)),
+            "point": tuple(s.point_xyz) if s.point_src else None, "rickerfc": s.rickerfc,
+            "src_index": cp(s.src_index, s.npts), "moment_rate": cp(s.moment_rate,
+                                                                   s.npts * s.src_nt * 6),
+            "src_nt": s.src_nt, "src_dt": s.src_dt,
+            "stations": cp(s.sta_xyz, 3 * s.nsta).reshape(-1, 3),
+        }
+    finally:
+        lib().cgfdm_free_setup(C.byref(s))
+    return out
+
+
+def run_directory(run_dir, precision=_lib.FP32, kernel=_lib.KERNEL_AUTO, device=0):
+    """The reference program on one GPU: reads run_dir, writes its outputs."""
+    check(lib().cgfdm_run_directory(run_dir.encode(), precision, kernel, device))
+
+
+__all__ = ["Simulation", "propagate", "setup_from_directory", "run_directory", "make_desc",
+           "device_bytes", "CgfdmError"]

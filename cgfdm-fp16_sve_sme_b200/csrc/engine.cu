@@ -1,0 +1,578 @@
+// Device state and time loop of one simulation (the body of propagate(),
+// propagate.cpp:24-228, on one GPU).
+//
+// Buffers (each 9 x num of storage type S, reference layout):
+//   A  wavefield at the start of a step; receives the step's result
+//   X, Y  RK stage ping-pong buffers
+//   T  RK4 accumulator
+// Stage mapping: irk0 A->X, irk1 X->Y, irk2 Y->X, irk3 X->A, with the RK
+// "m" state read from A (it is the step-start wavefield for stages 0-2, the
+// reference's m_W copy, wave_rk.cpp:29).  PML auxiliaries use the same
+// four-buffer scheme per slab.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <type_traits>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "kernels.h"
+
+namespace cgfdm {
+
+namespace {
+thread_local std::string g_err;
+}
+void set_error(const std::string &msg) { g_err = msg; }
+const char *last_error() { return g_err.c_str(); }
+
+#define CUDA_TRY(x)                                                                     \
+  do {                                                                                  \
+    cudaError_t e_ = (x);                                                               \
+    if (e_ != cudaSuccess) {                                                            \
+      set_error(std::string(#x) + ": " + cudaGetErrorString(e_));                       \
+      return e_ == cudaErrorMemoryAllocation ? CGFDM_ERR_NOMEM : CGFDM_ERR_CUDA;        \
+    }                                                                                   \
+  } while (0)
+
+namespace {
+
+static const int kFB[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1},  {-1, -1, 1},
+                              {-1, 1, -1},  {1, -1, -1}, {1, -1, 1}, {-1, 1, 1}};
+
+struct Dims {
+  int nx, ny, nz, npml;
+  int nx_, ny_, nz_;
+  long long num, nsurf;
+  long long slab_pts[5];
+  int slab_n[5][3], slab_off[5][3];
+};
+
+Dims make_dims(const cgfdm_desc &d) {
+  Dims m{};
+  m.nx = d.nx; m.ny = d.ny; m.nz = d.nz; m.npml = d.npml;
+  m.nx_ = d.nx + 2 * HALO; m.ny_ = d.ny + 2 * HALO; m.nz_ = d.nz + 2 * HALO;
+  m.num = (long long)m.nx_ * m.ny_ * m.nz_;
+  m.nsurf = (long long)m.nx_ * m.ny_;
+  for (int s = 0; s < 5; ++s) {
+    int ax = s % 3, flag = s >= 3;
+    int n[3] = {d.nx, d.ny, d.nz};
+    int off[3] = {HALO, HALO, HALO};
+    int full = n[ax];
+    n[ax] = d.npml;
+    off[ax] = HALO + flag * (full - d.npml);
+    for (int q = 0; q < 3; ++q) { m.slab_n[s][q] = n[q]; m.slab_off[s][q] = off[q]; }
+    m.slab_pts[s] = d.npml > 0 ? (long long)n[0] * n[1] * n[2] : 0;
+  }
+  return m;
+}
+
+template <typename S> class EngineT : public Engine {
+  using R = typename Arith<S>::R;
+
+ public:
+  explicit EngineT(const cgfdm_desc &d) : d_(d), g_(make_dims(d)) {}
+  ~EngineT() override { release(); }
+
+  int init() {
+    CUDA_TRY(cudaSetDevice(d_.device));
+    CUDA_TRY(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
+    const size_t wbytes = sizeof(S) * 9 * g_.num;
+    for (S **p : {&A_, &X_, &Y_, &T_}) {
+      CUDA_TRY(cudaMalloc(p, wbytes));
+      CUDA_TRY(cudaMemsetAsync(*p, 0, wbytes, own_stream_));
+    }
+    CUDA_TRY(cudaMalloc(&cjm_, sizeof(S) * 13 * g_.num));
+    CUDA_TRY(cudaMemsetAsync(cjm_, 0, sizeof(S) * 13 * g_.num, own_stream_));
+    CUDA_TRY(cudaMalloc(&rdz_, sizeof(R) * 18 * g_.nsurf));
+    CUDA_TRY(cudaMemsetAsync(rdz_, 0, sizeof(R) * 18 * g_.nsurf, own_stream_));
+    std::vector<float> prof = pml_profiles(g_.nx, g_.ny, g_.nz, g_.npml, d_.dh);
+    std::vector<R> profR(prof.begin(), prof.end());
+    CUDA_TRY(cudaMalloc(&pml_, sizeof(R) * profR.size()));
+    CUDA_TRY(cudaMemcpy(pml_, profR.data(), sizeof(R) * profR.size(), cudaMemcpyHostToDevice));
+    aux_total_ = 0;
+    for (int s = 0; s < 5; ++s) aux_total_ += g_.slab_pts[s] * 9;
+    if (aux_total_ > 0) {
+      CUDA_TRY(cudaMalloc(&aux_, sizeof(R) * 4 * aux_total_));
+      CUDA_TRY(cudaMemsetAsync(aux_, 0, sizeof(R) * 4 * aux_total_, own_stream_));
+    }
+    CUDA_TRY(cudaMalloc(&pgv_, sizeof(float) * 2 * (size_t)g_.nx * g_.ny));
+    CUDA_TRY(cudaMemsetAsync(pgv_, 0, sizeof(float) * 2 * (size_t)g_.nx * g_.ny, own_stream_));
+    CUDA_TRY(cudaMalloc(&amp343_, sizeof(float) * 343));
+    float amp[343];
+    gauss_weights343(amp);
+    CUDA_TRY(cudaMemcpy(amp343_, amp, sizeof amp, cudaMemcpyHostToDevice));
+    for (int q = 0; q < 6; ++q) CUDA_TRY(cudaEventCreate(&ev_[q]));
+    CUDA_TRY(cudaStreamSynchronize(own_stream_));
+    return CGFDM_OK;
+  }
+
+  int set_model(const float *cjm, const float *rdz) override {
+    CUDA_TRY(cudaSetDevice(d_.device));
+    CUDA_TRY(upload_converted(cjm, cjm_, 13 * g_.num));
+    std::vector<R> r(rdz, rdz + 18 * g_.nsurf);
+    CUDA_TRY(cudaMemcpy(rdz_, r.data(), sizeof(R) * r.size(), cudaMemcpyHostToDevice));
+    host_cjm_J_.assign(cjm + 9 * g_.num, cjm + 10 * g_.num);
+    host_cjm_mu_.assign(cjm + 10 * g_.num, cjm + 11 * g_.num);
+    model_set_ = true;
+    return CGFDM_OK;
+  }
+
+  int set_point_source(int sx, int sy, int sz, float rickerfc) override {
+    if (sx < HALO || sx >= g_.nx_ - HALO || sy < HALO || sy >= g_.ny_ - HALO || sz < HALO ||
+        sz >= g_.nz_ - HALO) {
+      // singleSource.cpp:157-164: a source outside the rank is skipped.
+      point_on_ = false;
+      return CGFDM_OK;
+    }
+    if (sx - 3 < 0 || sy - 3 < 0 || sz - 3 < 0 || sx + 3 >= g_.nx_ || sy + 3 >= g_.ny_ ||
+        sz + 3 >= g_.nz_) {
+      set_error("point source 7^3 smoothing window leaves the padded grid");
+      return CGFDM_ERR_SOURCE;
+    }
+    point_on_ = true;
+    psrc_[0] = sx; psrc_[1] = sy; psrc_[2] = sz;
+    rickerfc_ = rickerfc;
+    return CGFDM_OK;
+  }
+
+  int set_fault_source(const int64_t *idx, const float *rate, int64_t npts, int nt, float dt,
+                       bool scaled) override {
+    CUDA_TRY(cudaSetDevice(d_.device));
+    free_fault();
+    if (npts <= 0) { fault_on_ = false; return CGFDM_OK; }
+    for (int64_t p = 0; p < npts; ++p)
+      if (idx[p] < 0 || idx[p] >= g_.num) {
+        set_error("finite-fault cell index out of range");
+        return CGFDM_ERR_SOURCE;
+      }
+    std::vector<float> r(rate, rate + (size_t)npts * nt * 6);
+    if (!scaled) {
+      if (!model_set_) { set_error("set the model before an unscaled fault source"); return CGFDM_ERR_STATE; }
+      // calculate_MomentRate (addMoment.cpp:25-48)
+      const float DH = d_.dh;
+      for (int t = 0; t < nt; ++t)
+        for (int64_t p = 0; p < npts; ++p) {
+          float jacb = host_cjm_J_[idx[p]], mu = host_cjm_mu_[idx[p]];
+          float V = jacb * DH * DH * DH;
+          V = (float)(1.0 / V);
+          V = (float)(V * SCALE_OF<S>::cv);
+          float *m = &r[((size_t)t * npts + p) * 6];
+          for (int q = 0; q < 6; ++q) m[q] *= mu * V;
+        }
+    }
+    CUDA_TRY(cudaMalloc(&fidx_, sizeof(long long) * npts));
+    CUDA_TRY(cudaMemcpy(fidx_, idx, sizeof(long long) * npts, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMalloc(&frate_, sizeof(float) * r.size()));
+    CUDA_TRY(cudaMemcpy(frate_, r.data(), sizeof(float) * r.size(), cudaMemcpyHostToDevice));
+    fnpts_ = npts; fnt_ = nt; fdt_ = dt;
+    fault_on_ = true;
+    return CGFDM_OK;
+  }
+
+  int set_stations(const int32_t *xyz, int nsta) override {
+    CUDA_TRY(cudaSetDevice(d_.device));
+    if (sta_xyz_) { cudaFree(sta_xyz_); sta_xyz_ = nullptr; }
+    if (sta_wave_) { cudaFree(sta_wave_); sta_wave_ = nullptr; }
+    nsta_ = nsta;
+    if (nsta <= 0) return CGFDM_OK;
+    for (int s = 0; s < nsta; ++s) {
+      const int *q = xyz + 3 * s;
+      if (q[0] < HALO || q[0] >= g_.nx_ - HALO || q[1] < HALO || q[1] >= g_.ny_ - HALO ||
+          q[2] < HALO || q[2] >= g_.nz_ - HALO) {
+        set_error("station outside the interior grid");
+        return CGFDM_ERR_ARG;
+      }
+    }
+    CUDA_TRY(cudaMalloc(&sta_xyz_, sizeof(int) * 3 * nsta));
+    CUDA_TRY(cudaMemcpy(sta_xyz_, xyz, sizeof(int) * 3 * nsta, cudaMemcpyHostToDevice));
+    const size_t wb = sizeof(float) * (size_t)nsta * d_.nt * 9;
+    CUDA_TRY(cudaMalloc(&sta_wave_, wb));
+    CUDA_TRY(cudaMemsetAsync(sta_wave_, 0, wb, own_stream_));
+    CUDA_TRY(cudaStreamSynchronize(own_stream_));
+    return CGFDM_OK;
+  }
+
+  int run(int nsteps, void *stream) override {
+    CUDA_TRY(cudaSetDevice(d_.device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : own_stream_;
+    if (it_ + nsteps > d_.nt) {
+      set_error("run past the configured number of steps nt");
+      return CGFDM_ERR_ARG;
+    }
+    if (timing_) {
+      stage_used_ = 0;
+      CUDA_TRY(cudaEventRecord(ev_[0], st));
+    }
+    for (int s = 0; s < nsteps; ++s) {
+      const int it = it_;
+      // sources add into W once per step before stage 0 (propagate.cpp:145-151)
+      if (point_on_) {
+        float sm = ricker_moment(rickerfc_, it, d_.dt);
+        const float DH3 = d_.dh * d_.dh * d_.dh;
+        const double CsDT = SCALE_OF<S>::cs * (double)d_.dt;
+        CUDA_TRY(launch_point_source<S>(A_, X_, Y_, cjm_, g_.num, g_.nx_, g_.ny_, g_.nz_, psrc_[0],
+                                        psrc_[1], psrc_[2], amp343_, sm, DH3, CsDT, st));
+      }
+      if (fault_on_) {
+        // addMoment.cpp:238-264
+        float tmpT = (it + 0.0f) * d_.dt;
+        int srcIt = (int)(tmpT / fdt_);
+        if (srcIt + 1 >= fnt_) {
+          fault_on_ = false;
+        } else {
+          float t1 = float(srcIt) * fdt_;
+          float tw = (tmpT - t1) / fdt_;
+          CUDA_TRY(launch_fault_source<S>(A_, g_.num, fidx_, frate_, fnpts_, srcIt, tw, d_.dt, st));
+        }
+      }
+      int fb[3] = {kFB[it % 8][0], kFB[it % 8][1], kFB[it % 8][2]};
+      for (int irk = 0; irk < 4; ++irk) {
+        int rc = launch_stage(irk, fb, st);
+        if (rc) return rc;
+        fb[0] = -fb[0]; fb[1] = -fb[1]; fb[2] = -fb[2];
+      }
+      const float c1 = (float)(1.0 / SCALE_OF<S>::cv), c2 = (float)(1.0 / SCALE_OF<S>::cs);
+      CUDA_TRY(launch_station_pgv<S>(A_, g_.num, g_.nx_, g_.ny_, g_.nz_, sta_xyz_, nsta_, d_.nt, it,
+                                     sta_wave_, pgv_, c1, c2, 1.0 / SCALE_OF<S>::cv, st));
+      ++it_;
+    }
+    if (timing_) CUDA_TRY(cudaEventRecord(ev_[1], st));
+    last_stream_ = st;
+    return CGFDM_OK;
+  }
+
+  int stage(int irk, int fb1, int fb2, int fb3, void *stream) override {
+    CUDA_TRY(cudaSetDevice(d_.device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : own_stream_;
+    int fb[3] = {fb1, fb2, fb3};
+    last_stream_ = st;
+    return launch_stage(irk, fb, st);
+  }
+
+  int synchronize() override {
+    CUDA_TRY(cudaSetDevice(d_.device));
+    CUDA_TRY(cudaStreamSynchronize(own_stream_));
+    if (last_stream_) CUDA_TRY(cudaStreamSynchronize(last_stream_));
+    return CGFDM_OK;
+  }
+
+  int steps_done() const override { return it_; }
+
+  int get_stations(float *wave) override {
+    int rc = synchronize();
+    if (rc) return rc;
+    if (nsta_ > 0)
+      CUDA_TRY(cudaMemcpy(wave, sta_wave_, sizeof(float) * (size_t)nsta_ * d_.nt * 9,
+                          cudaMemcpyDeviceToHost));
+    return CGFDM_OK;
+  }
+
+  int get_pgv(float *pgv) override {
+    int rc = synchronize();
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpy(pgv, pgv_, sizeof(float) * 2 * (size_t)g_.nx * g_.ny, cudaMemcpyDeviceToHost));
+    return CGFDM_OK;
+  }
+
+  int get_wavefield(float *w) override { return download_converted(A_, w, 9 * g_.num); }
+
+  int get_free_surface(float *v3) override {
+    int rc = synchronize();
+    if (rc) return rc;
+    float *tmp = nullptr;
+    const size_t n = 3 * (size_t)g_.nx * g_.ny;
+    CUDA_TRY(cudaMalloc(&tmp, sizeof(float) * n));
+    cudaError_t e = launch_free_surface_pack<S>(A_, g_.num, g_.nx_, g_.ny_, g_.nz_,
+                                                1.0 / SCALE_OF<S>::cv, tmp, own_stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(v3, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost, own_stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(own_stream_);
+    cudaFree(tmp);
+    CUDA_TRY(e);
+    return CGFDM_OK;
+  }
+
+  int get_slice(int field, int axis, int at, double scale, float *out) override {
+    int rc = synchronize();
+    if (rc) return rc;
+    const size_t n = axis == 0 ? (size_t)g_.ny * g_.nz : axis == 1 ? (size_t)g_.nx * g_.nz
+                                                                    : (size_t)g_.nx * g_.ny;
+    float *tmp = nullptr;
+    CUDA_TRY(cudaMalloc(&tmp, sizeof(float) * n));
+    cudaError_t e = launch_slice_pack<S>(A_ + field * g_.num, g_.nx_, g_.ny_, g_.nz_, axis, at, scale,
+                                         tmp, own_stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost, own_stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(own_stream_);
+    cudaFree(tmp);
+    CUDA_TRY(e);
+    return CGFDM_OK;
+  }
+
+  int set_state(int irk, const float *W, const float *t, const float *m,
+                const float *aux) override {
+    // Places W in the input buffer of stage irk, m in the step-start buffer A
+    // (for irk 0 the stage input is A itself) and t in the accumulator.
+    CUDA_TRY(cudaSetDevice(d_.device));
+    if (irk < 0 || irk > 3) { set_error("irk must be 0..3"); return CGFDM_ERR_ARG; }
+    static const int in_of[4] = {0, 1, 2, 1};
+    S *bufs[3] = {A_, X_, Y_};
+    if (m && irk != 0) CUDA_TRY(upload_converted(m, A_, 9 * g_.num));
+    if (W) CUDA_TRY(upload_converted(W, bufs[in_of[irk]], 9 * g_.num));
+    if (t) CUDA_TRY(upload_converted(t, T_, 9 * g_.num));
+    if (aux && aux_total_ > 0) {
+      // host layout: per slab {Aux, t, m}
+      std::vector<R> a(aux_total_), tt(aux_total_), mm(aux_total_);
+      long long off = 0, dst = 0;
+      for (int s = 0; s < 5; ++s) {
+        long long n = g_.slab_pts[s] * 9;
+        for (long long q = 0; q < n; ++q) {
+          a[dst + q] = aux[off + q];
+          tt[dst + q] = aux[off + n + q];
+          mm[dst + q] = aux[off + 2 * n + q];
+        }
+        off += 3 * n;
+        dst += n;
+      }
+      if (irk != 0)
+        CUDA_TRY(cudaMemcpy(auxbuf(0), mm.data(), sizeof(R) * aux_total_, cudaMemcpyHostToDevice));
+      CUDA_TRY(cudaMemcpy(auxbuf(in_of[irk]), a.data(), sizeof(R) * aux_total_, cudaMemcpyHostToDevice));
+      CUDA_TRY(cudaMemcpy(auxbuf(3), tt.data(), sizeof(R) * aux_total_, cudaMemcpyHostToDevice));
+    }
+    return CGFDM_OK;
+  }
+
+  int get_state(float *W, float *t, float *m, float *aux) override {
+    int rc = synchronize();
+    if (rc) return rc;
+    if (W) { rc = download_converted(last_out_, W, 9 * g_.num); if (rc) return rc; }
+    if (t) { rc = download_converted(T_, t, 9 * g_.num); if (rc) return rc; }
+    if (m) { rc = download_converted(A_, m, 9 * g_.num); if (rc) return rc; }
+    if (aux && aux_total_ > 0) {
+      std::vector<R> o(aux_total_), tt(aux_total_), mm(aux_total_);
+      CUDA_TRY(cudaMemcpy(o.data(), last_aux_out_, sizeof(R) * aux_total_, cudaMemcpyDeviceToHost));
+      CUDA_TRY(cudaMemcpy(tt.data(), auxbuf(3), sizeof(R) * aux_total_, cudaMemcpyDeviceToHost));
+      CUDA_TRY(cudaMemcpy(mm.data(), auxbuf(0), sizeof(R) * aux_total_, cudaMemcpyDeviceToHost));
+      long long off = 0, src = 0;
+      for (int s = 0; s < 5; ++s) {
+        long long n = g_.slab_pts[s] * 9;
+        for (long long q = 0; q < n; ++q) {
+          aux[off + q] = (float)o[src + q];
+          aux[off + n + q] = (float)tt[src + q];
+          aux[off + 2 * n + q] = (float)mm[src + q];
+        }
+        off += 3 * n;
+        src += n;
+      }
+    }
+    return CGFDM_OK;
+  }
+
+  int64_t aux_floats() const override { return aux_total_; }
+
+  int set_timing(bool on) override { timing_ = on; return CGFDM_OK; }
+
+  int get_timing(float *ms3) override {
+    // [0] the last run() end to end, [1] sum over its stage-kernel launches,
+    // [2] the number of those launches
+    int rc = synchronize();
+    if (rc) return rc;
+    ms3[0] = ms3[1] = ms3[2] = 0.0f;
+    if (!timing_) return CGFDM_OK;
+    CUDA_TRY(cudaEventElapsedTime(&ms3[0], ev_[0], ev_[1]));
+    double sum = 0;
+    for (int q = 0; q < stage_used_; ++q) {
+      float ms = 0;
+      CUDA_TRY(cudaEventElapsedTime(&ms, stage_ev_[2 * q], stage_ev_[2 * q + 1]));
+      sum += ms;
+    }
+    ms3[1] = (float)sum;
+    ms3[2] = (float)stage_used_;
+    return CGFDM_OK;
+  }
+
+  const cgfdm_desc &desc() const override { return d_; }
+
+ private:
+  R *auxbuf(int b) const { return aux_ + (size_t)b * aux_total_; }
+
+  int launch_stage(int irk, const int fb[3], cudaStream_t st) {
+    // buffer roles of this stage (see the file comment)
+    static const int in_of[4] = {0, 1, 2, 1}, out_of[4] = {1, 2, 1, 0};
+    S *bufs[3] = {A_, X_, Y_};
+    StageArgs<S> a{};
+    a.win = bufs[in_of[irk]];
+    a.wout = bufs[out_of[irk]];
+    a.wm = A_;
+    a.t = T_;
+    a.cjm = cjm_;
+    a.rdz = rdz_;
+    a.pml = pml_;
+    a.nx_ = g_.nx_; a.ny_ = g_.ny_; a.nz_ = g_.nz_;
+    a.num = g_.num;
+    a.npml = g_.npml;
+    a.rDH = (float)(1.0 / d_.dh);
+    a.DT = d_.dt;
+    a.fb1 = fb[0]; a.fb2 = fb[1]; a.fb3 = fb[2];
+    a.irk = irk;
+    a.nslab = g_.npml > 0 ? 5 : 0;
+    size_t off = 0;
+    for (int s = 0; s < a.nslab; ++s) {
+      SlabDev<R> &sl = a.slab[s];
+      sl.n0 = g_.slab_n[s][0]; sl.n1 = g_.slab_n[s][1]; sl.n2 = g_.slab_n[s][2];
+      sl.off0 = g_.slab_off[s][0]; sl.off1 = g_.slab_off[s][1]; sl.off2 = g_.slab_off[s][2];
+      sl.axis = s % 3;
+      sl.ain = auxbuf(in_of[irk]) + off;
+      sl.aout = auxbuf(out_of[irk]) + off;
+      sl.am = auxbuf(0) + off;
+      sl.at = auxbuf(3) + off;
+      off += g_.slab_pts[s] * 9;
+    }
+    last_out_ = a.wout;
+    last_aux_out_ = auxbuf(out_of[irk]);
+    cudaError_t e = cudaSuccess;
+    const bool use_stream = d_.kernel == CGFDM_KERNEL_STREAM ||
+                            (d_.kernel == CGFDM_KERNEL_AUTO && stage_stream_supported<S>(a));
+    if (timing_) {
+      while ((int)stage_ev_.size() < 2 * (stage_used_ + 1)) {
+        cudaEvent_t ev;
+        CUDA_TRY(cudaEventCreate(&ev));
+        stage_ev_.push_back(ev);
+      }
+      CUDA_TRY(cudaEventRecord(stage_ev_[2 * stage_used_], st));
+    }
+    if (use_stream) e = launch_stage_stream<S>(a, st);
+    else e = launch_stage_exact<S>(a, st);
+    CUDA_TRY(e);
+    if (timing_) CUDA_TRY(cudaEventRecord(stage_ev_[2 * stage_used_++ + 1], st));
+    return CGFDM_OK;
+  }
+
+  cudaError_t upload_converted(const float *src, S *dst, long long n) {
+    if (std::is_same<S, float>::value)
+      return cudaMemcpy(dst, src, sizeof(float) * n, cudaMemcpyHostToDevice);
+    float *tmp = nullptr;
+    cudaError_t e = cudaMalloc(&tmp, sizeof(float) * n);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpy(tmp, src, sizeof(float) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_convert_in<S>(tmp, dst, n, own_stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(own_stream_);
+    cudaFree(tmp);
+    return e;
+  }
+
+  int download_converted(const S *src, float *dst, long long n) {
+    int rc = synchronize();
+    if (rc) return rc;
+    if (std::is_same<S, float>::value) {
+      CUDA_TRY(cudaMemcpy(dst, src, sizeof(float) * n, cudaMemcpyDeviceToHost));
+      return CGFDM_OK;
+    }
+    float *tmp = nullptr;
+    CUDA_TRY(cudaMalloc(&tmp, sizeof(float) * n));
+    cudaError_t e = launch_convert_out<S>(src, tmp, n, own_stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dst, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost, own_stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(own_stream_);
+    cudaFree(tmp);
+    CUDA_TRY(e);
+    return CGFDM_OK;
+  }
+
+  void free_fault() {
+    if (fidx_) cudaFree(fidx_);
+    if (frate_) cudaFree(frate_);
+    fidx_ = nullptr;
+    frate_ = nullptr;
+  }
+
+  void release() {
+    cudaSetDevice(d_.device);
+    if (own_stream_) cudaStreamSynchronize(own_stream_);
+    for (void *p : {(void *)A_, (void *)X_, (void *)Y_, (void *)T_, (void *)cjm_, (void *)rdz_,
+                    (void *)pml_, (void *)aux_, (void *)pgv_, (void *)amp343_, (void *)sta_xyz_,
+                    (void *)sta_wave_})
+      if (p) cudaFree(p);
+    free_fault();
+    for (auto &e : ev_)
+      if (e) cudaEventDestroy(e);
+    for (auto &e : stage_ev_) cudaEventDestroy(e);
+    if (own_stream_) cudaStreamDestroy(own_stream_);
+  }
+
+  cgfdm_desc d_;
+  Dims g_;
+  cudaStream_t own_stream_ = nullptr, last_stream_ = nullptr;
+  S *A_ = nullptr, *X_ = nullptr, *Y_ = nullptr, *T_ = nullptr, *cjm_ = nullptr;
+  R *rdz_ = nullptr, *pml_ = nullptr, *aux_ = nullptr;
+  long long aux_total_ = 0;
+  float *pgv_ = nullptr, *amp343_ = nullptr, *sta_wave_ = nullptr;
+  int *sta_xyz_ = nullptr;
+  int nsta_ = 0;
+  bool point_on_ = false, fault_on_ = false, model_set_ = false, timing_ = false;
+  int psrc_[3] = {0, 0, 0};
+  float rickerfc_ = 0;
+  long long *fidx_ = nullptr;
+  float *frate_ = nullptr;
+  long long fnpts_ = 0;
+  int fnt_ = 0;
+  float fdt_ = 0;
+  int it_ = 0;
+  S *last_out_ = nullptr;
+  R *last_aux_out_ = nullptr;
+  std::vector<float> host_cjm_J_, host_cjm_mu_;
+  cudaEvent_t ev_[6] = {};
+  std::vector<cudaEvent_t> stage_ev_;
+  int stage_used_ = 0;
+};
+
+}  // namespace
+
+int64_t engine_device_bytes(const cgfdm_desc &d) {
+  Dims g = make_dims(d);
+  int64_t s = d.precision == CGFDM_FP32 ? 4 : d.precision == CGFDM_FP64 ? 8 : 2;
+  int64_t r = d.precision == CGFDM_FP64 ? 8 : 4;
+  int64_t aux = 0;
+  for (int q = 0; q < 5; ++q) aux += g.slab_pts[q] * 9;
+  return s * (4 * 9 + 13) * g.num + r * (18 * g.nsurf + 4 * aux) + 8 * (int64_t)d.nx * d.ny;
+}
+
+int make_engine(const cgfdm_desc &d, std::unique_ptr<Engine> &out) {
+  if (d.nx <= 0 || d.ny <= 0 || d.nz <= 0 || d.nt < 0 || !(d.dh > 0) || !(d.dt > 0)) {
+    set_error("invalid grid descriptor");
+    return CGFDM_ERR_ARG;
+  }
+  if (d.nz < 4) {
+    set_error("nz must be at least 4 (three free-surface layers plus one interior layer)");
+    return CGFDM_ERR_ARG;
+  }
+  if (d.npml < 0 || d.npml > d.nx || d.npml > d.ny || d.npml > d.nz) {
+    set_error("the PML layer (nPML) is bigger than the grid");  // pml_deriv.cpp:53-59
+    return CGFDM_ERR_PML;
+  }
+  if (d.npml == 1) {
+    set_error("nPML must be 0 or at least 2 (the profile length is DH*(nPML-1))");
+    return CGFDM_ERR_PML;
+  }
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count <= d.device || d.device < 0) {
+    set_error("no CUDA device available for the CGFDM kernels");
+    return CGFDM_ERR_NO_KERNEL;
+  }
+  int rc = CGFDM_OK;
+  switch (d.precision) {
+    case CGFDM_FP32: { auto *e = new EngineT<float>(d); out.reset(e); rc = e->init(); } break;
+    case CGFDM_FP16: { auto *e = new EngineT<__half>(d); out.reset(e); rc = e->init(); } break;
+    case CGFDM_BF16: { auto *e = new EngineT<__nv_bfloat16>(d); out.reset(e); rc = e->init(); } break;
+    case CGFDM_FP64: { auto *e = new EngineT<double>(d); out.reset(e); rc = e->init(); } break;
+    default:
+      set_error("unknown precision");
+      return CGFDM_ERR_ARG;
+  }
+  if (rc) out.reset();
+  return rc;
+}
+
+}  // namespace cgfdm

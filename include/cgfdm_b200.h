@@ -1,0 +1,202 @@
+/*
+ * cgfdm_b200 -- B200-native (sm_100a) time-stepping hot path of CGFDM.
+ *
+ * C ABI: plain C types, host pointers and sizes only; every function returns a
+ * status code (CGFDM_OK = 0) instead of aborting.  A handle owns all device
+ * memory of one simulation; distinct handles may be driven from distinct host
+ * threads.  All array arguments are HOST memory unless stated otherwise.
+ *
+ * The reference entry point this library replaces is
+ *   void propagate(MPI_Comm, MPI_COORD, MPI_NEIGHBOR, GRID, PARAMS, WAVE,
+ *                  Mat_rDZ, FLOAT *CJM, SOURCE_FILE_INPUT, long long *srcIndex,
+ *                  float *momentRate, float *momentRateSlice, SLICE,
+ *                  SLICE_DATA, SLICE_DATA)
+ *   (src-new-FP32-SVE/functions.h:133-138, propagate.cpp:24-228), called once
+ *   from run() (run.cpp:142-146) on every MPI rank.  This library is the
+ *   single-rank drop-in: no halo exchange, the whole grid on one GPU.
+ *
+ * Array layouts are the reference's (XFAST, HALO = 3, padded dims
+ * _nx_ = nx + 6, _ny_ = ny + 6, _nz_ = nz + 6, num = _nx_*_ny_*_nz_):
+ *   cjm        13 x num float, fields xi_x xi_y xi_z et_x et_y et_z zt_x zt_y
+ *              zt_z J mu lambda buoyancy (CJM.cpp:117-131), mu/lambda/b already
+ *              converted (CJM.cpp:47-73)
+ *   rdz        2 x (_nx_*_ny_) x 9 float, _rDZ_DX then _rDZ_DY
+ *              (contravariant.cpp:179-198, 329-351)
+ *   wavefield  9 x num float: Vx Vy Vz Txx Tyy Tzz Txy Txz Tyz
+ *   stations   int32 [nsta][3] padded-grid indices (station.cpp:288-290);
+ *              output float [nsta][nt][9] (station.cpp:333-343)
+ *   pgv        float [ny][nx][2]: PGVh, PGV (PGV.cpp:80-99)
+ */
+#ifndef CGFDM_B200_H
+#define CGFDM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference's MPI_Abort codes where one exists) ---- */
+#define CGFDM_OK 0
+#define CGFDM_ERR_ARG 1            /* invalid argument / size */
+#define CGFDM_ERR_PARAMS 100       /* params.json missing/unparsable (getParams.cpp:23,46) */
+#define CGFDM_ERR_CFL 110          /* DT above the CFL limit (calc_CFL.cpp:341-344) */
+#define CGFDM_ERR_PML 130          /* nPML larger than the grid (pml_deriv.cpp:53-59) */
+#define CGFDM_ERR_NO_SOURCE 180    /* no source configured (modelChecking.cpp:37) */
+#define CGFDM_ERR_SOURCE 181       /* source outside the grid / unreadable source file */
+#define CGFDM_ERR_IO 200           /* file could not be read or written */
+#define CGFDM_ERR_CUDA 300         /* a CUDA runtime call failed */
+#define CGFDM_ERR_NOMEM 301        /* device memory budget exceeded at admission */
+#define CGFDM_ERR_NO_KERNEL 302    /* CUDA extension unusable (no device / wrong arch) */
+#define CGFDM_ERR_TIMEOUT 303      /* a bounded device-side wait expired */
+#define CGFDM_ERR_STATE 304        /* call not valid in the handle's current state */
+
+/* ---- storage precision of wavefield and coefficients ---- */
+#define CGFDM_FP32 0   /* float everywhere: the reference's FP32 build */
+#define CGFDM_FP16 1   /* scaled half storage, FP32 arithmetic (macro.h:65-73) */
+#define CGFDM_BF16 2   /* scaled bfloat16 storage, FP32 arithmetic */
+#define CGFDM_FP64 3   /* double everywhere: the accuracy oracle run */
+
+/* ---- kernel selection ---- */
+#define CGFDM_KERNEL_AUTO 0      /* fastest kernel for the precision */
+#define CGFDM_KERNEL_EXACT 1     /* reference operation order, no FMA contraction:
+                                    bit-identical to the reference's FP32 CPU path */
+#define CGFDM_KERNEL_STREAM 2    /* TMA-staged z-streaming fused stage kernel */
+
+typedef struct {
+  int32_t nx, ny, nz;     /* interior points (params NX, NY, NZ) */
+  int32_t npml;           /* PML thickness (params nPML); 0 disables the PML */
+  float dh;               /* grid spacing DH (m) */
+  float dt;               /* time step DT (s) */
+  int32_t nt;             /* number of steps NT = (int)(TMAX/DT) */
+  int32_t precision;      /* CGFDM_FP32 ... */
+  int32_t kernel;         /* CGFDM_KERNEL_* */
+  int32_t device;         /* CUDA device ordinal */
+} cgfdm_desc;
+
+typedef struct cgfdm_handle cgfdm_handle;
+
+/* Version / build identification; returns a static string. */
+const char *cgfdm_version(void);
+
+/* Text of the last error raised on the calling host thread. */
+const char *cgfdm_last_error(void);
+
+/* Device bytes a handle with this descriptor will hold (wavefield, RK
+ * buffers, coefficients, PML slabs), used for admission control. */
+int cgfdm_device_bytes(const cgfdm_desc *desc, int64_t *bytes);
+
+/* Creates a handle and allocates its device memory; the wavefield starts at
+ * rest (allocWave/allocPML zero-fill, wave_deriv.cpp:42, pml_deriv.cpp:26).
+ * Replaces the allocation half of propagate.cpp:65-92. */
+int cgfdm_create(const cgfdm_desc *desc, cgfdm_handle **out);
+int cgfdm_destroy(cgfdm_handle *h);
+
+/* Uploads the medium/metric coefficients and free-surface matrices in the
+ * reference layout (the CJM and mat_rDZ arguments of propagate()). */
+int cgfdm_set_model(cgfdm_handle *h, const float *cjm, const float *rdz);
+
+/* The smoothed explosive point source of singleSource.cpp:78-177 at padded
+ * indices (sx, sy, sz) with Ricker centre frequency rickerfc. */
+int cgfdm_set_point_source(cgfdm_handle *h, int32_t sx, int32_t sy, int32_t sz,
+                           float rickerfc);
+
+/* The finite-fault source of addMoment.cpp:222-339: npts cell indices
+ * (padded linear, the srcIndex argument of propagate()) and the moment-rate
+ * table momentRate [nt][npts][6] sampled at dt.  If `scaled` is 0 the
+ * table is scaled here by mu*Cv/(J*DH^3) (calculate_MomentRate,
+ * addMoment.cpp:12-65); pass 1 if it already is. */
+int cgfdm_set_fault_source(cgfdm_handle *h, const int64_t *src_index, const float *moment_rate,
+                           int64_t npts, int32_t nt, float dt, int32_t scaled);
+
+/* Station list (padded indices); seismograms are recorded every step. */
+int cgfdm_set_stations(cgfdm_handle *h, const int32_t *xyz, int32_t nsta);
+
+/* Advances nsteps time steps (sources, 4 RK stages, stations, PGV) on the
+ * CUDA stream `stream` (a cudaStream_t, NULL = the handle's own stream).
+ * Asynchronous: returns once the work is enqueued. */
+int cgfdm_run(cgfdm_handle *h, int32_t nsteps, void *stream);
+
+/* One RK stage irk (0..3) with MacCormack signs fb1..fb3 and no source,
+ * station or PGV work: the unit of the stage-level parity tests. */
+int cgfdm_stage(cgfdm_handle *h, int32_t irk, int32_t fb1, int32_t fb2, int32_t fb3,
+                void *stream);
+
+/* Waits for all work of the handle. */
+int cgfdm_synchronize(cgfdm_handle *h);
+
+/* Completed steps so far. */
+int cgfdm_steps_done(cgfdm_handle *h, int32_t *it);
+
+/* Host copies of results (blocking). */
+int cgfdm_get_stations(cgfdm_handle *h, float *wave);          /* [nsta][nt][9] */
+int cgfdm_get_pgv(cgfdm_handle *h, float *pgv);                /* [ny][nx][2]   */
+int cgfdm_get_wavefield(cgfdm_handle *h, float *w);            /* 9 x num       */
+/* Free-surface velocity snapshot (Vx, Vy, Vz on the top interior layer,
+ * data_io.cpp:481-491): float [3][ny][nx]. */
+int cgfdm_get_free_surface(cgfdm_handle *h, float *v3);
+
+/* Stage-test state access: the input W of stage irk, the RK accumulator t
+ * and (for irk 1..3) the step-start state m, each 9 x num; PML auxiliaries as
+ * 5 slabs (x1 y1 z1 x2 y2) x {Aux, t, m}, each [npos][9]
+ * (pml_deriv.cpp:12-32).  get_state returns the last stage's output W, t and
+ * m (m is the stage input for irk 0, as the reference's m_W copy). */
+int cgfdm_set_state(cgfdm_handle *h, int32_t irk, const float *W, const float *t,
+                    const float *m, const float *aux);
+int cgfdm_get_state(cgfdm_handle *h, float *W, float *t, float *m, float *aux);
+int cgfdm_aux_floats(cgfdm_handle *h, int64_t *n);   /* floats of one aux set */
+
+/* Device timing of the last cgfdm_run, from CUDA events on its stream (only
+ * when enabled with cgfdm_set_timing): [0] the whole run in ms, [1] the sum
+ * of the fused-stage kernel durations in ms, [2] the number of those stage
+ * launches. */
+int cgfdm_set_timing(cgfdm_handle *h, int32_t on);
+int cgfdm_get_timing(cgfdm_handle *h, float *ms3);
+
+/* Drop-in for propagate() with host buffers: uploads the model and sources,
+ * runs all nt steps, returns station seismograms, the PGV map and the final
+ * free-surface snapshot.  Any output pointer may be NULL. */
+int cgfdm_propagate(const cgfdm_desc *desc, const float *cjm, const float *rdz,
+                    int32_t point_src, const int32_t *point_xyz, float rickerfc,
+                    const int64_t *src_index, const float *moment_rate, int64_t npts,
+                    int32_t src_nt, float src_dt, const int32_t *sta_xyz, int32_t nsta,
+                    float *sta_out, float *pgv_out, float *freesurf_out);
+
+/* The reference program end to end (main.cpp -> run.cpp -> propagate.cpp) on
+ * one GPU: reads params.json / station.json / model files from run_dir,
+ * performs the setup on the host, runs the hot path here, and writes the
+ * reference's output files under params "out" (station_mpi_0_0_0.bin,
+ * PGV_Z_mpi_0_0_0.bin, V*_/FreeSurfV*_ slices, coord/medium slices). */
+int cgfdm_run_directory(const char *run_dir, int32_t precision, int32_t kernel,
+                        int32_t device);
+
+/* Host setup only (run.cpp:56-131 + propagate.cpp:65-128): builds the arrays
+ * the hot path consumes from the files in run_dir.  Buffers are allocated by
+ * the library and released with cgfdm_free_setup. */
+typedef struct {
+  cgfdm_desc desc;
+  float *cjm;             /* 13 x num */
+  float *rdz;             /* 2 x nsurf x 9 */
+  float *coord;           /* num x 3 (AoS, coord.cpp:137-139) */
+  float *medium;          /* num x 3 Vs Vp rho, before conversion */
+  float *pml;             /* alpha/beta/d x/y/z block (init_pml_para.cpp:21-51) */
+  int32_t point_src;      /* 1 if the single smoothed source is active */
+  int32_t point_xyz[3];
+  float rickerfc;
+  int64_t npts;           /* finite-fault cells after merging duplicates */
+  int32_t src_nt;
+  float src_dt;
+  int64_t *src_index;     /* [npts] */
+  float *moment_rate;     /* [src_nt][npts][6], scaled */
+  int32_t nsta;
+  int32_t *sta_xyz;       /* [nsta][3] padded */
+} cgfdm_setup;
+
+int cgfdm_setup_from_directory(const char *run_dir, cgfdm_setup *out);
+int cgfdm_free_setup(cgfdm_setup *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
