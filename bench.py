@@ -322,7 +322,9 @@ def main():
 
     sim = new_sim(total_steps)
     sim.set_timing(True)
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-null) stream: the work and the events share it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sim.run(args.warmup, stream.cuda_stream)
     torch.cuda.synchronize()
     if dist:

@@ -22,6 +22,36 @@ constexpr float kCf1 = -1.16666667f, kCf2 = 1.33333333f, kCf3 = -0.16666667f;
 constexpr float kB1 = 0.16666667f, kB2 = 0.33333333f, kB3 = 0.33333333f, kB4 = 0.16666667f,
                 kA2rk = 0.5f, kA3rk = 0.5f;
 
+// HBM layout of every 3-D field (wavefield components, coefficients): the
+// reference's padded grid (_nx_ x _ny_ x _nz_, halo 3, x fastest) with the
+// rows shifted by xoff elements and padded to a pitch that is a multiple of
+// 32 elements, so that the first interior column (i = 3) and every 32-column
+// tile origin i = 3 + 32 t start on a 128-byte boundary (whole L2 lines for
+// the tile loads and stores) and the halo box origin 16 bytes before it is a
+// legal TMA start.  The pad columns are zero.
+struct Layout {
+  int nx_, ny_, nz_;  // padded extents
+  int px;             // row pitch in elements
+  int xoff;           // row shift in elements
+  long long plane;    // px * ny_
+  long long fs;       // field stride (elements), a multiple of 32
+  __host__ __device__ __forceinline__ long long at(int i, int j, int k) const {
+    return (long long)(i + xoff) + (long long)j * px + (long long)k * plane;
+  }
+};
+
+__host__ __device__ inline Layout make_layout(int nx, int ny, int nz, int elem_bytes) {
+  Layout L;
+  L.nx_ = nx + 2 * HALO;
+  L.ny_ = ny + 2 * HALO;
+  L.nz_ = nz + 2 * HALO;
+  L.xoff = (128 / elem_bytes) - HALO;  // 29 (4-byte), 61 (2-byte), 13 (8-byte)
+  L.px = ((L.nx_ + L.xoff) + 31) / 32 * 32;
+  L.plane = (long long)L.px * L.ny_;
+  L.fs = (L.plane * L.nz_ + 31) / 32 * 32;
+  return L;
+}
+
 template <typename S> struct Arith { using R = float; };
 template <> struct Arith<double> { using R = double; };
 
@@ -57,17 +87,17 @@ template <typename A> struct SlabDev {
 
 // Everything one RK stage reads and writes.
 template <typename S> struct StageArgs {
-  const S *win;          // stage input wavefield, 9 x num
+  const S *win;          // stage input wavefield, 9 fields
   S *wout;               // stage output wavefield
   const S *wm;           // step-start wavefield (the RK "m" state)
-  S *t;                  // RK accumulator, 9 x num
-  const S *cjm;          // 13 x num
-  const typename Arith<S>::R *rdz;  // 2 x nsurf x 9 (_rDZ_DX then _rDZ_DY)
+  S *t;                  // RK accumulator
+  const S *cjm;          // 13 coefficient fields
+  const typename Arith<S>::R *rdz;  // 2 x (_nx_*_ny_) x 9 (_rDZ_DX then _rDZ_DY)
   const typename Arith<S>::R *pml;  // alpha, beta, d for x (nx_), y (ny_), z (nz_)
   SlabDev<typename Arith<S>::R> slab[5];  // x1 y1 z1 x2 y2
   int nslab;
-  int nx_, ny_, nz_;     // padded extents
-  long long num;
+  Layout L;
+  int kbeg, kend;        // padded z range of the points this launch updates
   int npml;
   float rDH, DT;
   int fb1, fb2, fb3, irk;

@@ -1,7 +1,8 @@
 // Device state and time loop of one simulation (the body of propagate(),
 // propagate.cpp:24-228, on one GPU).
 //
-// Buffers (each 9 x num of storage type S, reference layout):
+// Buffers (each 9 fields of storage type S in the HBM Layout of
+// device_common.cuh):
 //   A  wavefield at the start of a step; receives the step's result
 //   X, Y  RK stage ping-pong buffers
 //   T  RK4 accumulator
@@ -9,14 +10,18 @@
 // "m" state read from A (it is the step-start wavefield for stages 0-2, the
 // reference's m_W copy, wave_rk.cpp:29).  PML auxiliaries use the same
 // four-buffer scheme per slab.
+//
+// Kernel choice per stage: the TMA-staged streaming kernel updates the
+// planes below the three free-surface layers and the exact-order kernel the
+// top three layers (KERNEL_STREAM / AUTO); KERNEL_EXACT runs the exact-order
+// kernel everywhere (bit-identical to the reference's FP32 CPU build).
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
-#include <type_traits>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "engine.h"
@@ -41,12 +46,12 @@ const char *last_error() { return g_err.c_str(); }
 
 namespace {
 
-static const int kFB[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1},  {-1, -1, 1},
-                              {-1, 1, -1},  {1, -1, -1}, {1, -1, 1}, {-1, 1, 1}};
+const int kFB[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1},  {-1, -1, 1},
+                       {-1, 1, -1},  {1, -1, -1}, {1, -1, 1}, {-1, 1, 1}};
 
 struct Dims {
   int nx, ny, nz, npml;
-  int nx_, ny_, nz_;
+  Layout L;
   long long num, nsurf;
   long long slab_pts[5];
   int slab_n[5][3], slab_off[5][3];
@@ -55,9 +60,12 @@ struct Dims {
 Dims make_dims(const cgfdm_desc &d) {
   Dims m{};
   m.nx = d.nx; m.ny = d.ny; m.nz = d.nz; m.npml = d.npml;
-  m.nx_ = d.nx + 2 * HALO; m.ny_ = d.ny + 2 * HALO; m.nz_ = d.nz + 2 * HALO;
-  m.num = (long long)m.nx_ * m.ny_ * m.nz_;
-  m.nsurf = (long long)m.nx_ * m.ny_;
+  m.L = make_layout(d.nx, d.ny, d.nz,
+                    d.precision == CGFDM_FP16 || d.precision == CGFDM_BF16 ? 2
+                    : d.precision == CGFDM_FP64                            ? 8
+                                                                           : 4);
+  m.num = (long long)m.L.nx_ * m.L.ny_ * m.L.nz_;
+  m.nsurf = (long long)m.L.nx_ * m.L.ny_;
   for (int s = 0; s < 5; ++s) {
     int ax = s % 3, flag = s >= 3;
     int n[3] = {d.nx, d.ny, d.nz};
@@ -81,19 +89,19 @@ template <typename S> class EngineT : public Engine {
   int init() {
     CUDA_TRY(cudaSetDevice(d_.device));
     CUDA_TRY(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
-    const size_t wbytes = sizeof(S) * 9 * g_.num;
+    const size_t wbytes = sizeof(S) * 9 * g_.L.fs;
     for (S **p : {&A_, &X_, &Y_, &T_}) {
       CUDA_TRY(cudaMalloc(p, wbytes));
       CUDA_TRY(cudaMemsetAsync(*p, 0, wbytes, own_stream_));
     }
-    CUDA_TRY(cudaMalloc(&cjm_, sizeof(S) * 13 * g_.num));
-    CUDA_TRY(cudaMemsetAsync(cjm_, 0, sizeof(S) * 13 * g_.num, own_stream_));
+    CUDA_TRY(cudaMalloc(&cjm_, sizeof(S) * 13 * g_.L.fs));
+    CUDA_TRY(cudaMemsetAsync(cjm_, 0, sizeof(S) * 13 * g_.L.fs, own_stream_));
     CUDA_TRY(cudaMalloc(&rdz_, sizeof(R) * 18 * g_.nsurf));
     CUDA_TRY(cudaMemsetAsync(rdz_, 0, sizeof(R) * 18 * g_.nsurf, own_stream_));
     std::vector<float> prof = pml_profiles(g_.nx, g_.ny, g_.nz, g_.npml, d_.dh);
     std::vector<R> profR(prof.begin(), prof.end());
     CUDA_TRY(cudaMalloc(&pml_, sizeof(R) * profR.size()));
-    CUDA_TRY(cudaMemcpy(pml_, profR.data(), sizeof(R) * profR.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(h2d(pml_, profR.data(), sizeof(R) * profR.size()));
     aux_total_ = 0;
     for (int s = 0; s < 5; ++s) aux_total_ += g_.slab_pts[s] * 9;
     if (aux_total_ > 0) {
@@ -105,17 +113,33 @@ template <typename S> class EngineT : public Engine {
     CUDA_TRY(cudaMalloc(&amp343_, sizeof(float) * 343));
     float amp[343];
     gauss_weights343(amp);
-    CUDA_TRY(cudaMemcpy(amp343_, amp, sizeof amp, cudaMemcpyHostToDevice));
-    for (int q = 0; q < 6; ++q) CUDA_TRY(cudaEventCreate(&ev_[q]));
+    CUDA_TRY(h2d(amp343_, amp, sizeof amp));
+    // [0] device error flag of the streaming kernel, [1] its work-queue counter
+    CUDA_TRY(cudaMalloc(&err_flag_, 2 * sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(err_flag_, 0, 2 * sizeof(int), own_stream_));
+    for (int q = 0; q < 2; ++q) CUDA_TRY(cudaEventCreate(&ev_[q]));
+    use_stream_ = stage_stream_supported<S>() && d_.kernel != CGFDM_KERNEL_EXACT &&
+                  g_.nz > 3;
+    if (d_.kernel == CGFDM_KERNEL_STREAM && !stage_stream_supported<S>()) {
+      set_error("the streaming kernel does not support this precision");
+      return CGFDM_ERR_ARG;
+    }
+    if (use_stream_) {
+      S *bufs[3] = {A_, X_, Y_};
+      for (int b = 0; b < 3; ++b) {
+        int rc = encode_stream_maps<S>(bufs[b], cjm_, A_, T_, g_.L, tmap_[b]);
+        if (rc) return rc;
+      }
+    }
     CUDA_TRY(cudaStreamSynchronize(own_stream_));
     return CGFDM_OK;
   }
 
   int set_model(const float *cjm, const float *rdz) override {
     CUDA_TRY(cudaSetDevice(d_.device));
-    CUDA_TRY(upload_converted(cjm, cjm_, 13 * g_.num));
+    CUDA_TRY(upload_repacked(cjm, cjm_, 13));
     std::vector<R> r(rdz, rdz + 18 * g_.nsurf);
-    CUDA_TRY(cudaMemcpy(rdz_, r.data(), sizeof(R) * r.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(h2d(rdz_, r.data(), sizeof(R) * r.size()));
     host_cjm_J_.assign(cjm + 9 * g_.num, cjm + 10 * g_.num);
     host_cjm_mu_.assign(cjm + 10 * g_.num, cjm + 11 * g_.num);
     model_set_ = true;
@@ -123,14 +147,14 @@ template <typename S> class EngineT : public Engine {
   }
 
   int set_point_source(int sx, int sy, int sz, float rickerfc) override {
-    if (sx < HALO || sx >= g_.nx_ - HALO || sy < HALO || sy >= g_.ny_ - HALO || sz < HALO ||
-        sz >= g_.nz_ - HALO) {
-      // singleSource.cpp:157-164: a source outside the rank is skipped.
-      point_on_ = false;
+    const Layout &L = g_.L;
+    if (sx < HALO || sx >= L.nx_ - HALO || sy < HALO || sy >= L.ny_ - HALO || sz < HALO ||
+        sz >= L.nz_ - HALO) {
+      point_on_ = false;  // singleSource.cpp:157-164: a source outside the rank is skipped
       return CGFDM_OK;
     }
-    if (sx - 3 < 0 || sy - 3 < 0 || sz - 3 < 0 || sx + 3 >= g_.nx_ || sy + 3 >= g_.ny_ ||
-        sz + 3 >= g_.nz_) {
+    if (sx - 3 < 0 || sy - 3 < 0 || sz - 3 < 0 || sx + 3 >= L.nx_ || sy + 3 >= L.ny_ ||
+        sz + 3 >= L.nz_) {
       set_error("point source 7^3 smoothing window leaves the padded grid");
       return CGFDM_ERR_SOURCE;
     }
@@ -145,14 +169,24 @@ template <typename S> class EngineT : public Engine {
     CUDA_TRY(cudaSetDevice(d_.device));
     free_fault();
     if (npts <= 0) { fault_on_ = false; return CGFDM_OK; }
-    for (int64_t p = 0; p < npts; ++p)
+    const Layout &L = g_.L;
+    std::vector<long long> lidx(npts);
+    for (int64_t p = 0; p < npts; ++p) {
       if (idx[p] < 0 || idx[p] >= g_.num) {
         set_error("finite-fault cell index out of range");
         return CGFDM_ERR_SOURCE;
       }
-    std::vector<float> r(rate, rate + (size_t)npts * nt * 6);
+      const long long r = idx[p];
+      const int i = (int)(r % L.nx_), j = (int)((r / L.nx_) % L.ny_),
+                k = (int)(r / ((long long)L.nx_ * L.ny_));
+      lidx[p] = L.at(i, j, k);
+    }
+    std::vector<float> rr(rate, rate + (size_t)npts * nt * 6);
     if (!scaled) {
-      if (!model_set_) { set_error("set the model before an unscaled fault source"); return CGFDM_ERR_STATE; }
+      if (!model_set_) {
+        set_error("set the model before an unscaled fault source");
+        return CGFDM_ERR_STATE;
+      }
       // calculate_MomentRate (addMoment.cpp:25-48)
       const float DH = d_.dh;
       for (int t = 0; t < nt; ++t)
@@ -161,14 +195,14 @@ template <typename S> class EngineT : public Engine {
           float V = jacb * DH * DH * DH;
           V = (float)(1.0 / V);
           V = (float)(V * SCALE_OF<S>::cv);
-          float *m = &r[((size_t)t * npts + p) * 6];
+          float *m = &rr[((size_t)t * npts + p) * 6];
           for (int q = 0; q < 6; ++q) m[q] *= mu * V;
         }
     }
     CUDA_TRY(cudaMalloc(&fidx_, sizeof(long long) * npts));
-    CUDA_TRY(cudaMemcpy(fidx_, idx, sizeof(long long) * npts, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMalloc(&frate_, sizeof(float) * r.size()));
-    CUDA_TRY(cudaMemcpy(frate_, r.data(), sizeof(float) * r.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(h2d(fidx_, lidx.data(), sizeof(long long) * npts));
+    CUDA_TRY(cudaMalloc(&frate_, sizeof(float) * rr.size()));
+    CUDA_TRY(h2d(frate_, rr.data(), sizeof(float) * rr.size()));
     fnpts_ = npts; fnt_ = nt; fdt_ = dt;
     fault_on_ = true;
     return CGFDM_OK;
@@ -178,22 +212,24 @@ template <typename S> class EngineT : public Engine {
     CUDA_TRY(cudaSetDevice(d_.device));
     if (sta_xyz_) { cudaFree(sta_xyz_); sta_xyz_ = nullptr; }
     if (sta_wave_) { cudaFree(sta_wave_); sta_wave_ = nullptr; }
-    nsta_ = nsta;
+    nsta_ = 0;
     if (nsta <= 0) return CGFDM_OK;
+    const Layout &L = g_.L;
     for (int s = 0; s < nsta; ++s) {
       const int *q = xyz + 3 * s;
-      if (q[0] < HALO || q[0] >= g_.nx_ - HALO || q[1] < HALO || q[1] >= g_.ny_ - HALO ||
-          q[2] < HALO || q[2] >= g_.nz_ - HALO) {
+      if (q[0] < HALO || q[0] >= L.nx_ - HALO || q[1] < HALO || q[1] >= L.ny_ - HALO ||
+          q[2] < HALO || q[2] >= L.nz_ - HALO) {
         set_error("station outside the interior grid");
         return CGFDM_ERR_ARG;
       }
     }
     CUDA_TRY(cudaMalloc(&sta_xyz_, sizeof(int) * 3 * nsta));
-    CUDA_TRY(cudaMemcpy(sta_xyz_, xyz, sizeof(int) * 3 * nsta, cudaMemcpyHostToDevice));
+    CUDA_TRY(h2d(sta_xyz_, xyz, sizeof(int) * 3 * nsta));
     const size_t wb = sizeof(float) * (size_t)nsta * d_.nt * 9;
     CUDA_TRY(cudaMalloc(&sta_wave_, wb));
     CUDA_TRY(cudaMemsetAsync(sta_wave_, 0, wb, own_stream_));
     CUDA_TRY(cudaStreamSynchronize(own_stream_));
+    nsta_ = nsta;
     return CGFDM_OK;
   }
 
@@ -204,6 +240,7 @@ template <typename S> class EngineT : public Engine {
       set_error("run past the configured number of steps nt");
       return CGFDM_ERR_ARG;
     }
+    last_stream_ = st;
     if (timing_) {
       stage_used_ = 0;
       CUDA_TRY(cudaEventRecord(ev_[0], st));
@@ -215,8 +252,8 @@ template <typename S> class EngineT : public Engine {
         float sm = ricker_moment(rickerfc_, it, d_.dt);
         const float DH3 = d_.dh * d_.dh * d_.dh;
         const double CsDT = SCALE_OF<S>::cs * (double)d_.dt;
-        CUDA_TRY(launch_point_source<S>(A_, X_, Y_, cjm_, g_.num, g_.nx_, g_.ny_, g_.nz_, psrc_[0],
-                                        psrc_[1], psrc_[2], amp343_, sm, DH3, CsDT, st));
+        CUDA_TRY(launch_point_source<S>(A_, X_, Y_, cjm_, g_.L, psrc_[0], psrc_[1], psrc_[2],
+                                        amp343_, sm, DH3, CsDT, st));
       }
       if (fault_on_) {
         // addMoment.cpp:238-264
@@ -227,7 +264,7 @@ template <typename S> class EngineT : public Engine {
         } else {
           float t1 = float(srcIt) * fdt_;
           float tw = (tmpT - t1) / fdt_;
-          CUDA_TRY(launch_fault_source<S>(A_, g_.num, fidx_, frate_, fnpts_, srcIt, tw, d_.dt, st));
+          CUDA_TRY(launch_fault_source<S>(A_, g_.L.fs, fidx_, frate_, fnpts_, srcIt, tw, d_.dt, st));
         }
       }
       int fb[3] = {kFB[it % 8][0], kFB[it % 8][1], kFB[it % 8][2]};
@@ -237,12 +274,11 @@ template <typename S> class EngineT : public Engine {
         fb[0] = -fb[0]; fb[1] = -fb[1]; fb[2] = -fb[2];
       }
       const float c1 = (float)(1.0 / SCALE_OF<S>::cv), c2 = (float)(1.0 / SCALE_OF<S>::cs);
-      CUDA_TRY(launch_station_pgv<S>(A_, g_.num, g_.nx_, g_.ny_, g_.nz_, sta_xyz_, nsta_, d_.nt, it,
-                                     sta_wave_, pgv_, c1, c2, 1.0 / SCALE_OF<S>::cv, st));
+      CUDA_TRY(launch_station_pgv<S>(A_, g_.L, sta_xyz_, nsta_, d_.nt, it, sta_wave_, pgv_, c1, c2,
+                                     1.0 / SCALE_OF<S>::cv, st));
       ++it_;
     }
     if (timing_) CUDA_TRY(cudaEventRecord(ev_[1], st));
-    last_stream_ = st;
     return CGFDM_OK;
   }
 
@@ -258,6 +294,12 @@ template <typename S> class EngineT : public Engine {
     CUDA_TRY(cudaSetDevice(d_.device));
     CUDA_TRY(cudaStreamSynchronize(own_stream_));
     if (last_stream_) CUDA_TRY(cudaStreamSynchronize(last_stream_));
+    int flag = 0;
+    CUDA_TRY(cudaMemcpy(&flag, err_flag_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+      set_error("a bounded device-side wait of the streaming kernel expired");
+      return CGFDM_ERR_TIMEOUT;
+    }
     return CGFDM_OK;
   }
 
@@ -279,20 +321,14 @@ template <typename S> class EngineT : public Engine {
     return CGFDM_OK;
   }
 
-  int get_wavefield(float *w) override { return download_converted(A_, w, 9 * g_.num); }
+  int get_wavefield(float *w) override { return download_repacked(A_, w, 9); }
 
   int get_free_surface(float *v3) override {
-    int rc = synchronize();
-    if (rc) return rc;
-    float *tmp = nullptr;
-    const size_t n = 3 * (size_t)g_.nx * g_.ny;
-    CUDA_TRY(cudaMalloc(&tmp, sizeof(float) * n));
-    cudaError_t e = launch_free_surface_pack<S>(A_, g_.num, g_.nx_, g_.ny_, g_.nz_,
-                                                1.0 / SCALE_OF<S>::cv, tmp, own_stream_);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(v3, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost, own_stream_);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(own_stream_);
-    cudaFree(tmp);
-    CUDA_TRY(e);
+    const size_t n = (size_t)g_.nx * g_.ny;
+    for (int v = 0; v < 3; ++v) {
+      int rc = get_slice(v, 2, g_.L.nz_ - HALO - 1, 1.0 / SCALE_OF<S>::cv, v3 + v * n);
+      if (rc) return rc;
+    }
     return CGFDM_OK;
   }
 
@@ -303,8 +339,7 @@ template <typename S> class EngineT : public Engine {
                                                                     : (size_t)g_.nx * g_.ny;
     float *tmp = nullptr;
     CUDA_TRY(cudaMalloc(&tmp, sizeof(float) * n));
-    cudaError_t e = launch_slice_pack<S>(A_ + field * g_.num, g_.nx_, g_.ny_, g_.nz_, axis, at, scale,
-                                         tmp, own_stream_);
+    cudaError_t e = launch_slice_pack<S>(A_ + field * g_.L.fs, g_.L, axis, at, scale, tmp, own_stream_);
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost, own_stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(own_stream_);
     cudaFree(tmp);
@@ -320,9 +355,9 @@ template <typename S> class EngineT : public Engine {
     if (irk < 0 || irk > 3) { set_error("irk must be 0..3"); return CGFDM_ERR_ARG; }
     static const int in_of[4] = {0, 1, 2, 1};
     S *bufs[3] = {A_, X_, Y_};
-    if (m && irk != 0) CUDA_TRY(upload_converted(m, A_, 9 * g_.num));
-    if (W) CUDA_TRY(upload_converted(W, bufs[in_of[irk]], 9 * g_.num));
-    if (t) CUDA_TRY(upload_converted(t, T_, 9 * g_.num));
+    if (m && irk != 0) CUDA_TRY(upload_repacked(m, A_, 9));
+    if (W) CUDA_TRY(upload_repacked(W, bufs[in_of[irk]], 9));
+    if (t) CUDA_TRY(upload_repacked(t, T_, 9));
     if (aux && aux_total_ > 0) {
       // host layout: per slab {Aux, t, m}
       std::vector<R> a(aux_total_), tt(aux_total_), mm(aux_total_);
@@ -337,10 +372,9 @@ template <typename S> class EngineT : public Engine {
         off += 3 * n;
         dst += n;
       }
-      if (irk != 0)
-        CUDA_TRY(cudaMemcpy(auxbuf(0), mm.data(), sizeof(R) * aux_total_, cudaMemcpyHostToDevice));
-      CUDA_TRY(cudaMemcpy(auxbuf(in_of[irk]), a.data(), sizeof(R) * aux_total_, cudaMemcpyHostToDevice));
-      CUDA_TRY(cudaMemcpy(auxbuf(3), tt.data(), sizeof(R) * aux_total_, cudaMemcpyHostToDevice));
+      if (irk != 0) CUDA_TRY(h2d(auxbuf(0), mm.data(), sizeof(R) * aux_total_));
+      CUDA_TRY(h2d(auxbuf(in_of[irk]), a.data(), sizeof(R) * aux_total_));
+      CUDA_TRY(h2d(auxbuf(3), tt.data(), sizeof(R) * aux_total_));
     }
     return CGFDM_OK;
   }
@@ -348,10 +382,10 @@ template <typename S> class EngineT : public Engine {
   int get_state(float *W, float *t, float *m, float *aux) override {
     int rc = synchronize();
     if (rc) return rc;
-    if (W) { rc = download_converted(last_out_, W, 9 * g_.num); if (rc) return rc; }
-    if (t) { rc = download_converted(T_, t, 9 * g_.num); if (rc) return rc; }
-    if (m) { rc = download_converted(A_, m, 9 * g_.num); if (rc) return rc; }
-    if (aux && aux_total_ > 0) {
+    if (W && last_out_) { rc = download_repacked(last_out_, W, 9); if (rc) return rc; }
+    if (t) { rc = download_repacked(T_, t, 9); if (rc) return rc; }
+    if (m) { rc = download_repacked(A_, m, 9); if (rc) return rc; }
+    if (aux && aux_total_ > 0 && last_aux_out_) {
       std::vector<R> o(aux_total_), tt(aux_total_), mm(aux_total_);
       CUDA_TRY(cudaMemcpy(o.data(), last_aux_out_, sizeof(R) * aux_total_, cudaMemcpyDeviceToHost));
       CUDA_TRY(cudaMemcpy(tt.data(), auxbuf(3), sizeof(R) * aux_total_, cudaMemcpyDeviceToHost));
@@ -399,8 +433,15 @@ template <typename S> class EngineT : public Engine {
  private:
   R *auxbuf(int b) const { return aux_ + (size_t)b * aux_total_; }
 
+  // Host-to-device copy ordered on the handle's stream and complete on
+  // return (a plain cudaMemcpy from pageable memory may return before its
+  // DMA lands, and the handle's kernels run on a non-blocking stream).
+  cudaError_t h2d(void *dst, const void *src, size_t bytes) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, own_stream_);
+    return e == cudaSuccess ? cudaStreamSynchronize(own_stream_) : e;
+  }
+
   int launch_stage(int irk, const int fb[3], cudaStream_t st) {
-    // buffer roles of this stage (see the file comment)
     static const int in_of[4] = {0, 1, 2, 1}, out_of[4] = {1, 2, 1, 0};
     S *bufs[3] = {A_, X_, Y_};
     StageArgs<S> a{};
@@ -411,8 +452,7 @@ template <typename S> class EngineT : public Engine {
     a.cjm = cjm_;
     a.rdz = rdz_;
     a.pml = pml_;
-    a.nx_ = g_.nx_; a.ny_ = g_.ny_; a.nz_ = g_.nz_;
-    a.num = g_.num;
+    a.L = g_.L;
     a.npml = g_.npml;
     a.rDH = (float)(1.0 / d_.dh);
     a.DT = d_.dt;
@@ -432,10 +472,7 @@ template <typename S> class EngineT : public Engine {
       off += g_.slab_pts[s] * 9;
     }
     last_out_ = a.wout;
-    last_aux_out_ = auxbuf(out_of[irk]);
-    cudaError_t e = cudaSuccess;
-    const bool use_stream = d_.kernel == CGFDM_KERNEL_STREAM ||
-                            (d_.kernel == CGFDM_KERNEL_AUTO && stage_stream_supported<S>(a));
+    last_aux_out_ = aux_total_ > 0 ? auxbuf(out_of[irk]) : nullptr;
     if (timing_) {
       while ((int)stage_ev_.size() < 2 * (stage_used_ + 1)) {
         cudaEvent_t ev;
@@ -444,36 +481,43 @@ template <typename S> class EngineT : public Engine {
       }
       CUDA_TRY(cudaEventRecord(stage_ev_[2 * stage_used_], st));
     }
-    if (use_stream) e = launch_stage_stream<S>(a, st);
-    else e = launch_stage_exact<S>(a, st);
-    CUDA_TRY(e);
+    const int ksurf = g_.L.nz_ - HALO - 3;  // first of the three free-surface layers
+    if (use_stream_) {
+      StageArgs<S> b = a;
+      b.kbeg = HALO;
+      b.kend = ksurf;
+      CUDA_TRY(launch_stage_stream<S>(b, tmap_[in_of[irk]], err_flag_, err_flag_ + 1, st));
+      a.kbeg = ksurf;
+      a.kend = g_.L.nz_ - HALO;
+      CUDA_TRY(launch_stage_exact<S>(a, st));
+    } else {
+      a.kbeg = HALO;
+      a.kend = g_.L.nz_ - HALO;
+      CUDA_TRY(launch_stage_exact<S>(a, st));
+    }
     if (timing_) CUDA_TRY(cudaEventRecord(stage_ev_[2 * stage_used_++ + 1], st));
     return CGFDM_OK;
   }
 
-  cudaError_t upload_converted(const float *src, S *dst, long long n) {
-    if (std::is_same<S, float>::value)
-      return cudaMemcpy(dst, src, sizeof(float) * n, cudaMemcpyHostToDevice);
+  cudaError_t upload_repacked(const float *src, S *dst, int nfield) {
     float *tmp = nullptr;
+    const size_t n = (size_t)nfield * g_.num;
     cudaError_t e = cudaMalloc(&tmp, sizeof(float) * n);
     if (e != cudaSuccess) return e;
-    e = cudaMemcpy(tmp, src, sizeof(float) * n, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = launch_convert_in<S>(tmp, dst, n, own_stream_);
+    e = cudaMemcpyAsync(tmp, src, sizeof(float) * n, cudaMemcpyHostToDevice, own_stream_);
+    if (e == cudaSuccess) e = launch_repack_in<S>(tmp, dst, g_.L, nfield, own_stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(own_stream_);
     cudaFree(tmp);
     return e;
   }
 
-  int download_converted(const S *src, float *dst, long long n) {
+  int download_repacked(const S *src, float *dst, int nfield) {
     int rc = synchronize();
     if (rc) return rc;
-    if (std::is_same<S, float>::value) {
-      CUDA_TRY(cudaMemcpy(dst, src, sizeof(float) * n, cudaMemcpyDeviceToHost));
-      return CGFDM_OK;
-    }
     float *tmp = nullptr;
+    const size_t n = (size_t)nfield * g_.num;
     CUDA_TRY(cudaMalloc(&tmp, sizeof(float) * n));
-    cudaError_t e = launch_convert_out<S>(src, tmp, n, own_stream_);
+    cudaError_t e = launch_repack_out<S>(src, tmp, g_.L, nfield, own_stream_);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dst, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost, own_stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(own_stream_);
     cudaFree(tmp);
@@ -491,9 +535,10 @@ template <typename S> class EngineT : public Engine {
   void release() {
     cudaSetDevice(d_.device);
     if (own_stream_) cudaStreamSynchronize(own_stream_);
+    if (last_stream_) cudaStreamSynchronize(last_stream_);
     for (void *p : {(void *)A_, (void *)X_, (void *)Y_, (void *)T_, (void *)cjm_, (void *)rdz_,
                     (void *)pml_, (void *)aux_, (void *)pgv_, (void *)amp343_, (void *)sta_xyz_,
-                    (void *)sta_wave_})
+                    (void *)sta_wave_, (void *)err_flag_})
       if (p) cudaFree(p);
     free_fault();
     for (auto &e : ev_)
@@ -509,9 +554,10 @@ template <typename S> class EngineT : public Engine {
   R *rdz_ = nullptr, *pml_ = nullptr, *aux_ = nullptr;
   long long aux_total_ = 0;
   float *pgv_ = nullptr, *amp343_ = nullptr, *sta_wave_ = nullptr;
-  int *sta_xyz_ = nullptr;
+  int *sta_xyz_ = nullptr, *err_flag_ = nullptr;
   int nsta_ = 0;
-  bool point_on_ = false, fault_on_ = false, model_set_ = false, timing_ = false;
+  bool point_on_ = false, fault_on_ = false, model_set_ = false, timing_ = false,
+       use_stream_ = false;
   int psrc_[3] = {0, 0, 0};
   float rickerfc_ = 0;
   long long *fidx_ = nullptr;
@@ -523,7 +569,8 @@ template <typename S> class EngineT : public Engine {
   S *last_out_ = nullptr;
   R *last_aux_out_ = nullptr;
   std::vector<float> host_cjm_J_, host_cjm_mu_;
-  cudaEvent_t ev_[6] = {};
+  alignas(64) unsigned char tmap_[3][kStreamMapsBytes] = {};
+  cudaEvent_t ev_[2] = {};
   std::vector<cudaEvent_t> stage_ev_;
   int stage_used_ = 0;
 };
@@ -536,7 +583,7 @@ int64_t engine_device_bytes(const cgfdm_desc &d) {
   int64_t r = d.precision == CGFDM_FP64 ? 8 : 4;
   int64_t aux = 0;
   for (int q = 0; q < 5; ++q) aux += g.slab_pts[q] * 9;
-  return s * (4 * 9 + 13) * g.num + r * (18 * g.nsurf + 4 * aux) + 8 * (int64_t)d.nx * d.ny;
+  return s * (4 * 9 + 13) * g.L.fs + r * (18 * g.nsurf + 4 * aux) + 8 * (int64_t)d.nx * d.ny;
 }
 
 int make_engine(const cgfdm_desc &d, std::unique_ptr<Engine> &out) {

@@ -16,43 +16,55 @@ template <typename S> struct SCALE_OF { static constexpr double cv = 1.0, cs = 1
 template <> struct SCALE_OF<__half> { static constexpr double cv = 5.0e3, cs = 1.0e-6; };
 template <> struct SCALE_OF<__nv_bfloat16> { static constexpr double cv = 5.0e3, cs = 1.0e-6; };
 
+// Exact-order fused stage over the points kbeg <= k < kend (all i, j).
 template <typename S> cudaError_t launch_stage_exact(const StageArgs<S> &a, cudaStream_t st);
 
-// Streaming fused stage kernel (FP32/FP16/BF16 storage).
-template <typename S> cudaError_t launch_stage_stream(const StageArgs<S> &a, cudaStream_t st);
-template <typename S> bool stage_stream_supported(const StageArgs<S> &a);
+// TMA-staged z-streaming fused stage over kbeg <= k < kend, which must lie
+// below the three free-surface layers.  `maps` holds the tensor maps of the
+// stage input wavefield and of the coefficients (encode_stream_maps).
+constexpr int kStreamMapsBytes = 640;
+template <typename S>
+cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps, int *err_flag,
+                                int *work_counter, cudaStream_t st);
+template <typename S> bool stage_stream_supported();
+// Encodes the tensor maps the streaming kernel loads its tiles through (the
+// 9 wavefield components of the stage input `wave`, the 13 coefficient
+// fields of `cjm`, the step state `wm` and the RK accumulator `t`) into `out`
+// (kStreamMapsBytes, 64-byte aligned host memory).
+template <typename S>
+int encode_stream_maps(const S *wave, const S *cjm, const S *wm, const S *t, const Layout &L,
+                       void *out);
 
 // Smoothed point source (singleSource.cpp:78-127): adds value(cell) to
 // Txx, Tyy, Tzz of w0 and, for cells in the halo, of w1 and w2 too (halo
 // cells hold constant values that every stage buffer must share).
 template <typename S>
-cudaError_t launch_point_source(S *w0, S *w1, S *w2, const S *cjm, long long num, int nx_, int ny_,
-                                int nz_, int sx, int sy, int sz, const float *amp343, float s,
-                                float DH3, double CsDT, cudaStream_t st);
+cudaError_t launch_point_source(S *w0, S *w1, S *w2, const S *cjm, Layout L, int sx, int sy,
+                                int sz, const float *amp343, float s, float DH3, double CsDT,
+                                cudaStream_t st);
 
-// Finite-fault injection (addMoment.cpp:98-219, NO_SOURCE_SMOOTH).
+// Finite-fault injection (addMoment.cpp:98-219, NO_SOURCE_SMOOTH); idx are
+// offsets in the HBM layout.
 template <typename S>
-cudaError_t launch_fault_source(S *w, long long num, const long long *idx, const float *rate,
+cudaError_t launch_fault_source(S *w, long long fs, const long long *idx, const float *rate,
                                 long long npts, int srcIt, float tw, float DT, cudaStream_t st);
 
 // Station sampling (station.cpp:310-347) and PGV (PGV.cpp:49-101).
 template <typename S>
-cudaError_t launch_station_pgv(const S *w, long long num, int nx_, int ny_, int nz_, const int *xyz,
-                               int nsta, int NT, int it, float *wave, float *pgv, float c1, float c2,
-                               double cv_inv, cudaStream_t st);
+cudaError_t launch_station_pgv(const S *w, Layout L, const int *xyz, int nsta, int NT, int it,
+                               float *wave, float *pgv, float c1, float c2, double cv_inv,
+                               cudaStream_t st);
 
-// Top-layer velocity snapshot [3][ny][nx] (data_io.cpp:186-231 on the free
-// surface slice).
+// One field's interior slice at padded index `at` along axis 0/1/2, times
+// c (data_io.cpp:86-231).
 template <typename S>
-cudaError_t launch_free_surface_pack(const S *w, long long num, int nx_, int ny_, int nz_,
-                                     double cv_inv, float *out, cudaStream_t st);
-// Generic slice pack of one field: axis 0/1/2 at padded index `at`.
-template <typename S>
-cudaError_t launch_slice_pack(const S *field, int nx_, int ny_, int nz_, int axis, int at,
-                              double c, float *out, cudaStream_t st);
+cudaError_t launch_slice_pack(const S *field, Layout L, int axis, int at, double c, float *out,
+                              cudaStream_t st);
 
-// float <-> storage conversions on the device.
-template <typename S> cudaError_t launch_convert_in(const float *src, S *dst, long long n, cudaStream_t st);
-template <typename S> cudaError_t launch_convert_out(const S *src, float *dst, long long n, cudaStream_t st);
+// Reference layout (float, nfield x num) <-> HBM layout (S, nfield x fs).
+template <typename S>
+cudaError_t launch_repack_in(const float *src, S *dst, Layout L, int nfield, cudaStream_t st);
+template <typename S>
+cudaError_t launch_repack_out(const S *src, float *dst, Layout L, int nfield, cudaStream_t st);
 
 }  // namespace cgfdm

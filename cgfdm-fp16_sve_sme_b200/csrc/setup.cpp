@@ -4,7 +4,9 @@
 
 #include <sys/stat.h>
 
+#include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -67,6 +69,7 @@ int build_coord(const std::string &dir, Setup &s) {
   s.coord.assign(3 * s.num, 0.0f);
   s.terrain.assign(s.nsurf, 0.0f);
   const int NZ = p.NZ;
+  #pragma omp parallel for schedule(static)
   for (int k = 0; k < s.nz_; ++k)
     for (int j = 0; j < s.ny_; ++j)
       for (int i = 0; i < s.nx_; ++i) {
@@ -89,6 +92,7 @@ int build_coord(const std::string &dir, Setup &s) {
         float height = h * std::exp(-0.5f * (x * x / (a * a) + y * y / (b * b)));
         s.terrain[i + (long long)j * s.nx_] = height;
       }
+    #pragma omp parallel for schedule(static)
     for (int k = 0; k < s.nz_; ++k)
       for (int j = 0; j < s.ny_; ++j)
         for (int i = 0; i < s.nx_; ++i) {
@@ -110,6 +114,7 @@ int build_coord(const std::string &dir, Setup &s) {
     for (int j = 0; j < s.ny_; ++j)
       for (int i = 0; i < s.nx_; ++i) s.terrain[i + (long long)j * s.nx_] = g[i + (size_t)j * NXP];
     double Depth = p.Depth * 1e3;
+    #pragma omp parallel for schedule(static)
     for (int k = 0; k < s.nz_; ++k)
       for (int j = 0; j < s.ny_; ++j)
         for (int i = 0; i < s.nx_; ++i) {
@@ -134,6 +139,7 @@ uint64_t splitmix(uint64_t &x) {
 int build_medium(const std::string &dir, Setup &s) {
   const Params &p = s.p;
   s.medium.assign(3 * s.num, 0.0f);
+  #pragma omp parallel for schedule(static)
   for (long long q = 0; q < s.num; ++q) {
     s.medium[3 * q + 0] = 3464.0f;
     s.medium[3 * q + 1] = 6000.0f;
@@ -161,6 +167,7 @@ int build_medium(const std::string &dir, Setup &s) {
       rho[F] = row[3] * 1000.f;
     }
     const float tolerance = 1.0f;
+    #pragma omp parallel for schedule(static)
     for (int k = 0; k < s.nz_; ++k)
       for (int j = 0; j < s.ny_; ++j)
         for (int i = 0; i < s.nx_; ++i) {
@@ -185,8 +192,10 @@ int build_medium(const std::string &dir, Setup &s) {
   }
   if (p.mediumPerturbation != 0.0f) {
     // Extension: seeded uniform +-fraction perturbation of Vs and Vp per cell.
-    uint64_t st = 0x5EEDull ^ (uint64_t)(uint32_t)p.mediumSeed;
+    const uint64_t seed = 0x5EEDull ^ (uint64_t)(uint32_t)p.mediumSeed;
+    #pragma omp parallel for schedule(static)
     for (long long q = 0; q < s.num; ++q) {
+      uint64_t st = seed + (uint64_t)q * 0xD1B54A32D192ED03ull;
       double u = (splitmix(st) >> 11) * (1.0 / 9007199254740992.0);
       float f = (float)(1.0 + p.mediumPerturbation * (2.0 * u - 1.0));
       s.medium[3 * q] *= f;
@@ -213,6 +222,7 @@ double distance_point2plane(const double P[3], const double A[3], const double B
 // calc_CFL (calc_CFL.cpp:265-363): smallest cell height against Vp max.
 int check_cfl(const Setup &s) {
   double hmin = 1.0e20;
+  #pragma omp parallel for schedule(dynamic, 1) reduction(min : hmin)
   for (int k = H; k < s.nz_ - H; ++k)
     for (int j = H; j < s.ny_ - H; ++j)
       for (int i = H; i < s.nx_ - H; ++i) {
@@ -231,6 +241,7 @@ int check_cfl(const Setup &s) {
       }
   float H_min = (float)hmin;
   float vpmax = -1.0e20f;
+  #pragma omp parallel for reduction(max : vpmax)
   for (long long q = 0; q < s.num; ++q)
     if (s.medium[3 * q + 1] > vpmax) vpmax = s.medium[3 * q + 1];
   float dtmax = 1.34 * H_min / vpmax;
@@ -250,6 +261,7 @@ void build_cjm(Setup &s, const Scale &sc) {
   const long long num = s.num;
   std::vector<float> med = s.medium;  // converted copy
   const double c = 1.0 * sc.Cs / sc.Cv;
+  #pragma omp parallel for schedule(static)
   for (long long q = 0; q < num; ++q) {
     float Vs = med[3 * q], Vp = med[3 * q + 1];
     float rho = med[3 * q + 2] * c;
@@ -269,6 +281,7 @@ void build_cjm(Setup &s, const Scale &sc) {
             kA2 * C[(idx + 2 * o) * 3 + var] + kA3 * C[(idx + 3 * o) * 3 + var]) *
            rDH;
   };
+  #pragma omp parallel for schedule(dynamic, 1)
   for (int k = H; k < s.nz_ - H; ++k)
     for (int j = H; j < s.ny_ - H; ++j)
       for (int i = H; i < s.nx_ - H; ++i) {
@@ -301,6 +314,7 @@ void build_cjm(Setup &s, const Scale &sc) {
   s.rdz.assign(18 * s.nsurf, 0.0f);
   const int ktop = s.nz_ - H - 1;
   float *DXo = s.rdz.data(), *DYo = s.rdz.data() + 9 * s.nsurf;
+  #pragma omp parallel for schedule(static)
   for (int k = ktop; k < s.nz_; ++k)
     for (int j = H; j < s.ny_ - H; ++j)
       for (int i = H; i < s.nx_ - H; ++i) {
@@ -366,6 +380,7 @@ void build_cjm(Setup &s, const Scale &sc) {
         }
       }
   s.cjm.assign(13 * num, 0.0f);  // set_CJM (CJM.cpp:106-134)
+  #pragma omp parallel for schedule(static)
   for (long long q = 0; q < num; ++q) {
     for (int v = 0; v < 9; ++v) s.cjm[q + num * v] = con[9 * q + v];
     s.cjm[q + num * 9] = Jac[q];
@@ -587,10 +602,24 @@ int build_setup(const std::string &dir, int precision, Setup &s) {
   d.kernel = CGFDM_KERNEL_AUTO;
   d.device = 0;
   const Scale sc = scale_of(precision);
+  // CGFDM_VERBOSE=1 prints the duration of each setup phase to stderr
+  const bool verbose = std::getenv("CGFDM_VERBOSE") != nullptr;
+  auto t0 = std::chrono::steady_clock::now();
+  auto phase = [&](const char *name) {
+    if (!verbose) return;
+    auto t1 = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[cgfdm setup] %-8s %.2f s\n", name,
+                 std::chrono::duration<double>(t1 - t0).count());
+    t0 = t1;
+  };
   if ((rc = build_coord(dir, s))) return rc;
+  phase("coord");
   if ((rc = build_medium(dir, s))) return rc;
+  phase("medium");
   if ((rc = check_cfl(s))) return rc;
+  phase("cfl");
   build_cjm(s, sc);
+  phase("cjm");
   s.pml = pml_profiles(p.NX, p.NY, p.NZ, p.nPML, (float)p.DH);
   if (p.useSingleSource) {
     int sx = p.sourceX + H, sy = p.sourceY + H, sz = p.sourceZ + H;  // locateSource

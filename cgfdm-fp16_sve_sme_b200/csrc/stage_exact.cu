@@ -78,16 +78,17 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
   using R = typename Arith<S>::R;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + HALO;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + HALO;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z + HALO;
-  if (i >= a.nx_ - HALO || j >= a.ny_ - HALO || k >= a.nz_ - HALO) return;
-  const long long num = a.num;
-  const long long sx = 1, sy = a.nx_, sz = (long long)a.nx_ * a.ny_;
-  const long long c = i + j * sy + k * sz;
-  const int ktop = a.nz_ - HALO - 1;  // top interior layer (_nz - 1)
+  const int k = blockIdx.z * blockDim.z + threadIdx.z + a.kbeg;
+  const int nx_ = a.L.nx_, ny_ = a.L.ny_, nz_ = a.L.nz_;
+  if (i >= nx_ - HALO || j >= ny_ - HALO || k >= a.kend) return;
+  const long long num = a.L.fs;  // field stride
+  const long long sx = 1, sy = a.L.px, sz = a.L.plane;
+  const long long c = a.L.at(i, j, k);
+  const int ktop = nz_ - HALO - 1;  // top interior layer (_nz - 1)
   const R rDH = a.rDH, DT = a.DT;
   const S *W = a.win;
   const S *cjm = a.cjm;
-  const R *px = a.pml, *py = a.pml + 3 * a.nx_, *pz = a.pml + 3 * a.nx_ + 3 * a.ny_;
+  const R *px = a.pml, *py = a.pml + 3 * nx_, *pz = a.pml + 3 * nx_ + 3 * ny_;
   const R mu = ldv(cjm + c + num * 10), lam = ldv(cjm + c + num * 11);
   const R b = ldv(cjm + c + num * 12);  // buoyancy already includes 1/Crho; *Crho below
   const int fbv[3] = {a.fb1, a.fb2, a.fb3};
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
 
   if (k < ktop - 2) {
     // wave_deriv.cpp:116-201
-    const R beta[3] = {px[a.nx_ + i], py[a.ny_ + j], pz[a.nz_ + k]};
+    const R beta[3] = {px[nx_ + i], py[ny_ + j], pz[nz_ + k]};
     const R bu = b * (R)CRHO_OF<S>::v;
     R term[3][9];
 #pragma unroll
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
     for (int v = 0; v < 9; ++v) h[v] = rnd<S>((term[0][v] + term[1][v] + term[2][v]) * DT);
   } else {
     // free_surface_deriv (freeSurface.cpp:104-256)
-    const R bx = px[a.nx_ + i], by = py[a.ny_ + j];
+    const R bx = px[nx_ + i], by = py[ny_ + j];
     const R bu = b * (R)CRHO_OF<S>::v;
     const int ks = ktop - k + HALO;
     R jx[3][7], jy[3][7], jz[3][7], r[3];
@@ -145,9 +146,9 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
       vet[v] = Lop(W + v * num, c, sy, a.fb2, rDH) * by;
     }
     if (k == ktop) {
-      const long long s2 = i + (long long)j * a.nx_;
+      const long long s2 = i + (long long)j * nx_;
       const R *DX = a.rdz + s2 * 9;
-      const R *DY = a.rdz + (long long)a.nx_ * a.ny_ * 9 + s2 * 9;
+      const R *DY = a.rdz + (long long)nx_ * ny_ * 9 + s2 * 9;
 #pragma unroll
       for (int q = 0; q < 3; ++q)
         vzt[q] = (DX[3 * q] * vxi[0] + DX[3 * q + 1] * vxi[1] + DX[3 * q + 2] * vxi[2]) +
@@ -186,7 +187,7 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
     const int ax = sl.axis;
     const int l = ax == 0 ? i : ax == 1 ? j : k;
     const R *prof = ax == 0 ? px : ax == 1 ? py : pz;
-    const int nax = ax == 0 ? a.nx_ : ax == 1 ? a.ny_ : a.nz_;
+    const int nax = ax == 0 ? nx_ : ax == 1 ? ny_ : nz_;
     const R alpha = prof[l], bt = prof[nax + l], dl = prof[2 * nax + l];
     const R ad = dl + alpha;
     const long long pos = i0 + (long long)j0 * sl.n0 + (long long)k0 * sl.n0 * sl.n1;
@@ -206,8 +207,8 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
     }
     if (k == ktop && ax != 2) {
       // pml_freeSurface.cpp: surface-gradient correction of the stress aux
-      const long long s2 = i + (long long)j * a.nx_;
-      const R *M = a.rdz + (ax == 0 ? 0 : (long long)a.nx_ * a.ny_ * 9) + s2 * 9;
+      const long long s2 = i + (long long)j * nx_;
+      const R *M = a.rdz + (ax == 0 ? 0 : (long long)nx_ * ny_ * 9) + s2 * 9;
       R vd[3], vz[3], zt[3], t[9];
       const R z6[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
@@ -279,7 +280,8 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
 
 template <typename S> cudaError_t launch_stage_exact(const StageArgs<S> &a, cudaStream_t st) {
   dim3 block(32, 4, 2);
-  dim3 grid((a.nx_ - 2 * HALO + 31) / 32, (a.ny_ - 2 * HALO + 3) / 4, (a.nz_ - 2 * HALO + 1) / 2);
+  if (a.kend <= a.kbeg) return cudaSuccess;
+  dim3 grid((a.L.nx_ - 2 * HALO + 31) / 32, (a.L.ny_ - 2 * HALO + 3) / 4, (a.kend - a.kbeg + 1) / 2);
   stage_exact_kernel<S><<<grid, block, 0, st>>>(a);
   return cudaGetLastError();
 }

@@ -1,22 +1,656 @@
-// Streaming fused stage kernel: placeholder until the TMA-staged kernel
-// lands; reports itself unsupported so the exact kernel runs.
+// TMA-staged z-streaming fused RK stage (the fast path).
+//
+// Persistent CTAs (one 512-thread CTA per SM) pull work items from an atomic
+// queue; an item is a 32 x 16 column tile and a chunk of z planes, ordered so
+// that concurrently running items are neighbours at the same depth (their
+// halo rows meet in L2).  Within an item the CTA sweeps z against the
+// MacCormack z direction (upward when FB3 = -1, downward when FB3 = +1), so
+// the one-sided z stencil of output plane k only needs plane k + dir beyond
+// it: a 5-plane register window per thread holds the z stencil, and shared
+// memory holds three rings fed by 4-D TMA tile loads (cp.async.bulk.tensor,
+// no multicast), each slot guarded by an mbarrier:
+//   W ring (3): the 9 wavefield components of one input plane with the x/y
+//               halo of the one-sided stencils (x origin 16-byte aligned);
+//   C ring (2): the 9 metrics and (mu, lambda, buoyancy) of one output plane;
+//   M ring (2): the RK step state m and accumulator t of one output plane
+//               (stages that read them).
+// Every operand of the stage therefore arrives asynchronously ahead of use;
+// only the PML auxiliaries (a minority of points) are read with plain loads.
+// Derivative, elastic combination, PML ADE update and the RK4 combination of
+// wavefield and auxiliaries are fused: each field is read and written once
+// per stage, stores are whole 128-byte lines per warp row.
+//
+// Arithmetic: FP32 with FMA contraction; the sign FB and 1/DH are folded into
+// the stencil weights and each direction's elastic combination is formed once
+// and scaled by the PML beta (main update) and d (auxiliary update), equal to
+// the reference up to rounding.  The three free-surface layers are left to
+// the exact-order kernel.
+//
+// Every mbarrier wait is bounded (2^31 clock cycles); on expiry the CTA sets
+// the error flag, drains the copies it issued (again bounded) and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <type_traits>
+
+#include "engine.h"
 #include "kernels.h"
 
 namespace cgfdm {
+namespace {
 
-template <typename S> bool stage_stream_supported(const StageArgs<S> &) { return false; }
+constexpr int TX = 32, TY = 16, NTHR = TX * TY;
+constexpr int BY = TY + 4;  // y box: 1 or 3 rows before the tile, 3 or 1 after
+constexpr long long kWaitCycles = 1LL << 31;
 
-template <typename S> cudaError_t launch_stage_stream(const StageArgs<S> &, cudaStream_t) {
+template <typename S> struct Geo {
+  static constexpr int ES = (int)sizeof(S);
+  static constexpr int HB = 16 / ES;                             // elements per 16 bytes
+  static constexpr int BX = ((HB + TX + 3) + HB - 1) / HB * HB;  // x box, aligned origin
+  static constexpr int W_BYTES = ((9 * BY * BX * ES) + 127) / 128 * 128;
+  static constexpr int C_BYTES = 12 * NTHR * ES;                 // 9 metrics + mu, lambda, b
+  static constexpr int M_BYTES = 18 * NTHR * ES;                 // m (9) and t (9)
+  static constexpr int NW = ES == 4 ? 3 : 4;
+  static constexpr int NC = ES == 4 ? 2 : 3;
+  static constexpr int NM = ES == 4 ? 2 : 3;
+  static constexpr int OFF_C = NW * W_BYTES;
+  static constexpr int OFF_M = OFF_C + NC * C_BYTES;
+  static constexpr int OFF_BAR = OFF_M + NM * M_BYTES;
+  static constexpr int SMEM = OFF_BAR + 8 * (NW + NC + NM) + 128;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(1000000u)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > kWaitCycles) return false;
+  return true;
+}
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                            int z, int f, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(f), "r"(bar)
+      : "memory");
+}
+
+// Elastic combination of one direction from its raw derivatives
+// (wave_deriv.cpp:163-191 without the PML factor): m = metric row,
+// L = d(Vx,Vy,Vz,Txx,Tyy,Tzz,Txy,Txz,Tyz).  Velocity rows include b.
+__device__ __forceinline__ void elastic9(const float m[3], const float L[9], float mu, float lam,
+                                         float b, float E[9]) {
+  E[0] = (m[0] * L[3] + m[1] * L[6] + m[2] * L[7]) * b;
+  E[1] = (m[0] * L[6] + m[1] * L[4] + m[2] * L[8]) * b;
+  E[2] = (m[0] * L[7] + m[1] * L[8] + m[2] * L[5]) * b;
+  const float mvx = m[0] * L[0], mvy = m[1] * L[1], mvz = m[2] * L[2];
+  const float div = (mvx + mvy + mvz) * lam;
+  const float tmu = 2.0f * mu;
+  E[3] = div + tmu * mvx;
+  E[4] = div + tmu * mvy;
+  E[5] = div + tmu * mvz;
+  E[6] = (m[1] * L[0] + m[0] * L[1]) * mu;
+  E[7] = (m[2] * L[0] + m[0] * L[2]) * mu;
+  E[8] = (m[2] * L[1] + m[1] * L[2]) * mu;
+}
+
+// PML auxiliary update of one slab point (pml_deriv.cpp:199-237, pml_rk.cpp)
+// given the direction's elastic combination E; adds -beta*Aux*DT into hc.
+__device__ __forceinline__ void pml_point(const SlabDev<float> &sl, long long pos, const float E[9],
+                                          float dl, float ad, float bt, float DT, int irk,
+                                          float hc[9]) {
+  const float *ain = sl.ain + pos * 9;
+  float *aout = sl.aout + pos * 9;
+  float *at = sl.at + pos * 9;
+  const float *am = sl.am + pos * 9;
+#pragma unroll
+  for (int v = 0; v < 9; ++v) {
+    const float a = ain[v];
+    const float ha = (dl * E[v] - ad * a) * DT;
+    hc[v] -= bt * a * DT;
+    switch (irk) {
+      case 0:
+        at[v] = a + kB1 * ha;
+        aout[v] = a + kA2rk * ha;
+        break;
+      case 1:
+        at[v] = at[v] + kB2 * ha;
+        aout[v] = am[v] + kA3rk * ha;
+        break;
+      case 2:
+        at[v] = at[v] + kB3 * ha;
+        aout[v] = am[v] + ha;
+        break;
+      default:
+        aout[v] = at[v] + kB4 * ha;
+    }
+  }
+}
+
+__device__ __forceinline__ long long slab_pos(const SlabDev<float> &sl, int i, int j, int k) {
+  return (i - sl.off0) + (long long)(j - sl.off1) * sl.n0 + (long long)(k - sl.off2) * sl.n0 * sl.n1;
+}
+
+struct Maps {
+  CUtensorMap w;   // stage input wavefield, box BX x BY x 1 x 9
+  CUtensorMap c9;  // coefficients, box 32 x 16 x 1 x 9 (metrics)
+  CUtensorMap c3;  // coefficients, box 32 x 16 x 1 x 3 (mu, lambda, b at field 10)
+  CUtensorMap m;   // step-start wavefield, box 32 x 16 x 1 x 9
+  CUtensorMap t;   // RK accumulator, box 32 x 16 x 1 x 9
+};
+
+struct Work {
+  int ntx, nty, nchunk, chunk, nitems;
+  int *counter;
+};
+
+template <typename S, int FB1, int FB2, int FB3>
+__global__ void __launch_bounds__(NTHR, 1)
+    stage_stream_kernel(const __grid_constant__ Maps maps, const StageArgs<S> a, const Work wk,
+                        int *err) {
+  using G = Geo<S>;
+  constexpr int NW = G::NW, NC = G::NC, NM = G::NM, BX = G::BX;
+  constexpr int DIR = -FB3;  // sweep direction in z
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  uint64_t *bw = (uint64_t *)(smem + G::OFF_BAR);
+  uint64_t *bc = bw + NW;
+  uint64_t *bm = bc + NC;
+  __shared__ int s_item, s_bad;
+
+  const int tid = threadIdx.x;
+  const int c = tid % TX, r = tid / TX;
+  const Layout L = a.L;
+  const int irk = a.irk;
+  const bool need_m = irk == 1 || irk == 2, need_t = irk >= 1;
+  const uint32_t m_bytes = (need_m ? 9 : 0) * NTHR * G::ES + (need_t ? 9 : 0) * NTHR * G::ES;
+  const float rDH = a.rDH, DT = a.DT;
+  // stencil weights with the MacCormack sign and 1/DH folded in
+  const float wx[5] = {FB1 * kAm1 * rDH, FB1 * kA0 * rDH, FB1 * kA1 * rDH, FB1 * kA2 * rDH, FB1 * kA3 * rDH};
+  const float wy[5] = {FB2 * kAm1 * rDH, FB2 * kA0 * rDH, FB2 * kA1 * rDH, FB2 * kA2 * rDH, FB2 * kA3 * rDH};
+  const float wz[5] = {FB3 * kAm1 * rDH, FB3 * kA0 * rDH, FB3 * kA1 * rDH, FB3 * kA2 * rDH, FB3 * kA3 * rDH};
+  const float *px = a.pml, *py = a.pml + 3 * L.nx_, *pz = a.pml + 3 * L.nx_ + 3 * L.ny_;
+  const long long fs = L.fs;
+  const int cidx = r * TX + c;
+
+  if (tid == 0) {
+    s_bad = 0;
+    for (int s = 0; s < NW + NC + NM; ++s) mbar_init(smem_u32(&bw[s]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  // ring fill counters, continued across work items
+  unsigned fw0 = 0, fc0 = 0, fm0 = 0;
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(wk.counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= wk.nitems || s_bad) break;
+    const int tile = item % (wk.ntx * wk.nty), chk = item / (wk.ntx * wk.nty);
+    const int bxi = tile % wk.ntx, byi = tile / wk.ntx;
+    const int kb = a.kbeg + chk * wk.chunk;
+    const int ke = min(kb + wk.chunk, a.kend);
+    const int nout = ke - kb, nplanes = nout + 4;
+    const int q0 = DIR > 0 ? kb - 3 : ke + 2;  // input planes q_n = q0 + n*DIR
+    const int i = HALO + bxi * TX + c, j = HALO + byi * TY + r;
+    const bool valid = i < L.nx_ - HALO && j < L.ny_ - HALO;
+    const int tx0 = HALO + L.xoff + bxi * TX;  // HBM x of the tile's first column
+    const int wx0 = tx0 - G::HB;
+    const int wy0 = HALO + byi * TY - (FB2 > 0 ? 1 : 3);
+    const int ty0 = HALO + byi * TY;
+    const int xs = c + G::HB, ys = r + (FB2 > 0 ? 1 : 3);
+
+    auto issue_w = [&](int n) {
+      const unsigned f = fw0 + n, s = f % NW;
+      const uint32_t bar = smem_u32(&bw[s]);
+      mbar_expect_tx(bar, 9 * BY * BX * G::ES);
+      tma_load_4d(smem_u32(smem + s * G::W_BYTES), &maps.w, wx0, wy0, q0 + n * DIR, 0, bar);
+    };
+    auto issue_c = [&](int o) {  // output o is plane kb + o (DIR > 0) or ke-1-o
+      const unsigned f = fc0 + o, s = f % NC;
+      const int k = DIR > 0 ? kb + o : ke - 1 - o;
+      const uint32_t bar = smem_u32(&bc[s]);
+      unsigned char *dst = smem + G::OFF_C + s * G::C_BYTES;
+      mbar_expect_tx(bar, G::C_BYTES);
+      tma_load_4d(smem_u32(dst), &maps.c9, tx0, ty0, k, 0, bar);
+      tma_load_4d(smem_u32(dst + 9 * NTHR * G::ES), &maps.c3, tx0, ty0, k, 10, bar);
+    };
+    auto issue_m = [&](int o) {
+      const unsigned f = fm0 + o, s = f % NM;
+      const int k = DIR > 0 ? kb + o : ke - 1 - o;
+      const uint32_t bar = smem_u32(&bm[s]);
+      unsigned char *dst = smem + G::OFF_M + s * G::M_BYTES;
+      mbar_expect_tx(bar, m_bytes);
+      if (need_m) tma_load_4d(smem_u32(dst), &maps.m, tx0, ty0, k, 0, bar);
+      if (need_t) tma_load_4d(smem_u32(dst + 9 * NTHR * G::ES), &maps.t, tx0, ty0, k, 0, bar);
+    };
+    if (tid == 0) {
+      for (int n = 0; n < NW - 1 && n < nplanes; ++n) issue_w(n);
+      for (int o = 0; o < NC && o < nout; ++o) issue_c(o);
+      if (need_t)
+        for (int o = 0; o < NM && o < nout; ++o) issue_m(o);
+    }
+
+    // per-column PML beta times DT (the auxiliaries are updated by pml_correct_kernel)
+    const int ic = valid ? i : HALO, jc = valid ? j : HALO;
+    const float bxd = px[L.nx_ + ic] * DT, byd = py[L.ny_ + jc] * DT;
+
+    // z window in registers: physical slot n mod 5 holds input plane q_n; the
+    // plane loop is unrolled five times so that every slot index is a
+    // compile-time constant and the window rotates without register moves.
+    float win[9][5];
+#pragma unroll
+    for (int v = 0; v < 9; ++v)
+#pragma unroll
+      for (int m = 0; m < 5; ++m) win[v][m] = 0.0f;
+
+    // one input plane with window rotation R = n mod 5; false on a failed wait
+    auto iter = [&](auto Rc, const int n) -> bool {
+      constexpr int R = decltype(Rc)::value;
+      constexpr int P0 = R, P1 = (R + 4) % 5, P2 = (R + 3) % 5, P3 = (R + 2) % 5, P4 = (R + 1) % 5;
+      const int o = n - 4;  // output index of this iteration (o < 0: window warm-up)
+      bool ok = mbar_wait_bounded(smem_u32(&bw[(fw0 + n) % NW]), ((fw0 + n) / NW) & 1);
+      if (o >= 0) {
+        ok = ok && mbar_wait_bounded(smem_u32(&bc[(fc0 + o) % NC]), ((fc0 + o) / NC) & 1);
+        if (need_t) ok = ok && mbar_wait_bounded(smem_u32(&bm[(fm0 + o) % NM]), ((fm0 + o) / NM) & 1);
+      }
+      if (!ok) {
+        s_bad = 1;
+        atomicExch(err, 1);
+      }
+      __syncthreads();
+      if (s_bad) return false;
+      const S *tq = (const S *)(smem + ((fw0 + n) % NW) * G::W_BYTES);
+#pragma unroll
+      for (int v = 0; v < 9; ++v) win[v][P0] = ldv(tq + (v * BY + ys) * BX + xs);
+      if (o >= 0 && valid) {
+        const int k = q0 + n * DIR - DIR;
+        const S *xy = (const S *)(smem + ((fw0 + n + NW - 1) % NW) * G::W_BYTES);  // plane k
+        const S *cf = (const S *)(smem + G::OFF_C + ((fc0 + o) % NC) * G::C_BYTES);
+        float mx[3], my[3], mz[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          mx[q] = ldv(cf + q * NTHR + cidx);
+          my[q] = ldv(cf + (3 + q) * NTHR + cidx);
+          mz[q] = ldv(cf + (6 + q) * NTHR + cidx);
+        }
+        const float mu = ldv(cf + 9 * NTHR + cidx), lam = ldv(cf + 10 * NTHR + cidx);
+        const float bu = ldv(cf + 11 * NTHR + cidx) * (float)CRHO_OF<S>::v;
+        const float bzd = pz[L.nz_ + k] * DT;
+        float h[9], Lr[9], E[9];
+        // x direction
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+          const S *row = xy + (v * BY + ys) * BX + xs;
+          Lr[v] = wx[0] * ldv(row - FB1) + wx[1] * ldv(row) + wx[2] * ldv(row + FB1) +
+                  wx[3] * ldv(row + 2 * FB1) + wx[4] * ldv(row + 3 * FB1);
+        }
+        elastic9(mx, Lr, mu, lam, bu, E);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) h[v] = bxd * E[v];
+        // y direction
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+          const S *col = xy + (v * BY + ys) * BX + xs;
+          Lr[v] = wy[0] * ldv(col - FB2 * BX) + wy[1] * ldv(col) + wy[2] * ldv(col + FB2 * BX) +
+                  wy[3] * ldv(col + 2 * FB2 * BX) + wy[4] * ldv(col + 3 * FB2 * BX);
+        }
+        elastic9(my, Lr, mu, lam, bu, E);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) h[v] += byd * E[v];
+        // z direction: W[k - m*DIR] for m = -1..3 sits in slots P0 (q = k + DIR) .. P4
+#pragma unroll
+        for (int v = 0; v < 9; ++v)
+          Lr[v] = wz[0] * win[v][P0] + wz[1] * win[v][P1] + wz[2] * win[v][P2] +
+                  wz[3] * win[v][P3] + wz[4] * win[v][P4];
+        elastic9(mz, Lr, mu, lam, bu, E);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) h[v] += bzd * E[v];
+        // RK4 combination (wave_rk.cpp:13-99)
+        const S *ms = (const S *)(smem + G::OFF_M + ((fm0 + o) % NM) * G::M_BYTES);
+        const S *ts = ms + 9 * NTHR;
+        const long long ctr = L.at(i, j, k);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+          const float hv = h[v];
+          const long long q = ctr + v * fs;
+          switch (irk) {
+            case 0: {
+              const float m0 = win[v][P1];  // the stage input at k is the step state
+              stv(a.t + q, m0 + kB1 * hv);
+              stv(a.wout + q, m0 + kA2rk * hv);
+            } break;
+            case 1:
+              stv(a.t + q, ldv(ts + v * NTHR + cidx) + kB2 * hv);
+              stv(a.wout + q, ldv(ms + v * NTHR + cidx) + kA3rk * hv);
+              break;
+            case 2:
+              stv(a.t + q, ldv(ts + v * NTHR + cidx) + kB3 * hv);
+              stv(a.wout + q, ldv(ms + v * NTHR + cidx) + hv);
+              break;
+            default:
+              stv(a.wout + q, ldv(ts + v * NTHR + cidx) + kB4 * hv);
+          }
+        }
+      }
+      __syncthreads();  // every thread is done with W plane n-1, C and M slot of o
+      if (tid == 0) {
+        if (n + NW - 1 < nplanes) issue_w(n + NW - 1);
+        if (o >= 0 && o + NC < nout) issue_c(o + NC);
+        if (o >= 0 && need_t && o + NM < nout) issue_m(o + NM);
+      }
+      return true;
+    };
+    int n = 0;
+    while (n < nplanes) {
+      if (!iter(std::integral_constant<int, 0>{}, n)) break;
+      if (++n >= nplanes) break;
+      if (!iter(std::integral_constant<int, 1>{}, n)) break;
+      if (++n >= nplanes) break;
+      if (!iter(std::integral_constant<int, 2>{}, n)) break;
+      if (++n >= nplanes) break;
+      if (!iter(std::integral_constant<int, 3>{}, n)) break;
+      if (++n >= nplanes) break;
+      if (!iter(std::integral_constant<int, 4>{}, n)) break;
+      ++n;
+    }
+    if (n < nplanes) {
+      // error exit: drain what was issued and not yet waited for (bounded)
+      if (tid == 0) {
+        for (int m = n + 1; m < nplanes && m < n + NW - 1; ++m)
+          mbar_wait_bounded(smem_u32(&bw[(fw0 + m) % NW]), ((fw0 + m) / NW) & 1);
+        const int o = n - 4 > 0 ? n - 4 : 0;
+        for (int m = o; m < nout && m < o + NC; ++m)
+          mbar_wait_bounded(smem_u32(&bc[(fc0 + m) % NC]), ((fc0 + m) / NC) & 1);
+        if (need_t)
+          for (int m = o; m < nout && m < o + NM; ++m)
+            mbar_wait_bounded(smem_u32(&bm[(fm0 + m) % NM]), ((fm0 + m) / NM) & 1);
+      }
+      break;
+    }
+    fw0 += nplanes;
+    fc0 += nout;
+    if (need_t) fm0 += nout;
+  }
+}
+
+// PML of the streaming path, applied after the streaming kernel to the slab
+// points below the free-surface layers (pml_deriv.cpp:90-544, pml_rk.cpp).
+// For each point of the slabs of one axis: the raw derivative of the stage
+// input along that axis, its elastic combination E, the ADE update of the
+// auxiliaries and their RK4 step, and the -beta*Aux*DT correction added to
+// the already written stage outputs (the RK4 combination is linear in h:
+// wout += a_irk * corr, t += b_irk * corr).  x and y have two disjoint slabs
+// each; launches per axis run in sequence, so points in several slabs
+// (edges, corners) receive the corrections one after the other.
+template <typename S>
+__global__ void __launch_bounds__(256) pml_correct_kernel(const StageArgs<S> a, int axis, int kend) {
+  const Layout L = a.L;
+  const int nsl = axis == 2 ? 1 : 2;
+  const SlabDev<float> &s0 = a.slab[axis];
+  const long long per = (long long)s0.n0 * s0.n1 * (kend - s0.off2 < s0.n2 ? kend - s0.off2 : s0.n2);
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (per <= 0 || t >= per * nsl) return;
+  const int which = (int)(t / per);
+  const SlabDev<float> &sl = a.slab[axis + 3 * which];
+  const long long p = t % per;
+  const int i0 = (int)(p % sl.n0), j0 = (int)((p / sl.n0) % sl.n1), k0 = (int)(p / ((long long)sl.n0 * sl.n1));
+  const int i = sl.off0 + i0, j = sl.off1 + j0, k = sl.off2 + k0;
+  if (k >= kend) return;
+  const long long pos = i0 + (long long)j0 * sl.n0 + (long long)k0 * sl.n0 * sl.n1;
+  const long long fs = L.fs, c = L.at(i, j, k);
+  const long long o = axis == 0 ? 1 : axis == 1 ? L.px : L.plane;
+  const int fb = axis == 0 ? a.fb1 : axis == 1 ? a.fb2 : a.fb3;
+  const int irk = a.irk;
+  const float w0 = fb * kAm1 * a.rDH, w1 = fb * kA0 * a.rDH, w2 = fb * kA1 * a.rDH,
+              w3 = fb * kA2 * a.rDH, w4 = fb * kA3 * a.rDH;
+  const long long q = fb * o;
+  // every load first (the outputs and auxiliaries are rewritten below)
+  const float *__restrict__ ain = sl.ain + pos * 9;
+  const float *__restrict__ am = sl.am + pos * 9;
+  float *__restrict__ aout = sl.aout + pos * 9;
+  float *__restrict__ at = sl.at + pos * 9;
+  S *__restrict__ wo = a.wout + c;
+  S *__restrict__ tw = a.t + c;
+  float av[9], amv[9], atv[9], wov[9], twv[9], Lr[9];
+#pragma unroll
+  for (int v = 0; v < 9; ++v) {
+    av[v] = ain[v];
+    amv[v] = (irk == 1 || irk == 2) ? am[v] : 0.0f;
+    atv[v] = irk >= 1 ? at[v] : 0.0f;
+    wov[v] = ldv(wo + v * fs);
+    twv[v] = irk < 3 ? (float)ldv(tw + v * fs) : 0.0f;
+    const S *w = a.win + v * fs + c;
+    Lr[v] = w0 * ldv(w - q) + w1 * ldv(w) + w2 * ldv(w + q) + w3 * ldv(w + 2 * q) + w4 * ldv(w + 3 * q);
+  }
+  float m[3], E[9];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) m[d] = ldv(a.cjm + c + (3 * axis + d) * fs);
+  const float mu = ldv(a.cjm + c + 10 * fs), lam = ldv(a.cjm + c + 11 * fs);
+  const float bu = ldv(a.cjm + c + 12 * fs) * (float)CRHO_OF<S>::v;
+  elastic9(m, Lr, mu, lam, bu, E);
+  const float *prof = a.pml + (axis == 0 ? 0 : axis == 1 ? 3 * L.nx_ : 3 * (L.nx_ + L.ny_));
+  const int nax = axis == 0 ? L.nx_ : axis == 1 ? L.ny_ : L.nz_;
+  const int l = axis == 0 ? i : axis == 1 ? j : k;
+  const float dl = prof[2 * nax + l], bt = prof[nax + l], ad = prof[l] + dl;
+  const float DT = a.DT;
+  float ca, cb;
+  switch (irk) {
+    case 0: ca = kA2rk; cb = kB1; break;
+    case 1: ca = kA3rk; cb = kB2; break;
+    case 2: ca = 1.0f; cb = kB3; break;
+    default: ca = kB4; cb = 0.0f;
+  }
+#pragma unroll
+  for (int v = 0; v < 9; ++v) {
+    const float x = av[v];
+    const float ha = (dl * E[v] - ad * x) * DT;  // pml_deriv.cpp:199-207
+    const float corr = -bt * x * DT;             // pml_deriv.cpp:219-227
+    switch (irk) {                               // pml_rk.cpp:15-69
+      case 0:
+        at[v] = x + kB1 * ha;
+        aout[v] = x + kA2rk * ha;
+        break;
+      case 1:
+        at[v] = atv[v] + kB2 * ha;
+        aout[v] = amv[v] + kA3rk * ha;
+        break;
+      case 2:
+        at[v] = atv[v] + kB3 * ha;
+        aout[v] = amv[v] + ha;
+        break;
+      default:
+        aout[v] = atv[v] + kB4 * ha;
+    }
+    stv(wo + v * fs, wov[v] + ca * corr);
+    if (irk < 3) stv(tw + v * fs, twv[v] + cb * corr);
+  }
+}
+
+template <typename S, int FB1, int FB2, int FB3>
+cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *counter,
+                       cudaStream_t st) {
+  static int attr_dev = -1;
+  auto kern = stage_stream_kernel<S, FB1, FB2, FB3>;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    cudaError_t e =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Geo<S>::SMEM);
+    if (e != cudaSuccess) return e;
+    attr_dev = dev;
+  }
+  static int nsm = 0;
+  if (!nsm) {
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (nsm <= 0) nsm = 148;
+  }
+  const int nx = a.L.nx_ - 2 * HALO, ny = a.L.ny_ - 2 * HALO;
+  Work wk;
+  wk.ntx = (nx + TX - 1) / TX;
+  wk.nty = (ny + TY - 1) / TY;
+  const int tiles = wk.ntx * wk.nty;
+  const int planes = a.kend - a.kbeg;
+  // about 24 items per SM, chunks of at least 24 planes
+  int nchunk = (24 * nsm + tiles - 1) / tiles;
+  nchunk = std::max(1, std::min(nchunk, planes / 24));
+  wk.chunk = (planes + nchunk - 1) / nchunk;
+  wk.nchunk = (planes + wk.chunk - 1) / wk.chunk;
+  wk.nitems = tiles * wk.nchunk;
+  wk.counter = counter;
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  const int grid = std::min(wk.nitems, nsm);
+  kern<<<grid, NTHR, Geo<S>::SMEM, st>>>(maps, a, wk, err);
+  return cudaGetLastError();
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+template <typename S> CUtensorMapDataType dtype_of();
+template <> CUtensorMapDataType dtype_of<float>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT32; }
+template <> CUtensorMapDataType dtype_of<__half>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT16; }
+template <> CUtensorMapDataType dtype_of<__nv_bfloat16>() { return CU_TENSOR_MAP_DATA_TYPE_BFLOAT16; }
+
+// 4-D map (x, y, z, field) over nfield fields of the HBM layout with the
+// given box.
+template <typename S>
+int encode_map(const S *base, const Layout &L, int nfield, int bx, int by, int bf, CUtensorMap *m) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled is unavailable in this driver");
+    return CGFDM_ERR_NO_KERNEL;
+  }
+  const cuuint64_t es = sizeof(S);
+  cuuint64_t dims[4] = {(cuuint64_t)L.px, (cuuint64_t)L.ny_, (cuuint64_t)L.nz_, (cuuint64_t)nfield};
+  cuuint64_t strides[3] = {(cuuint64_t)L.px * es, (cuuint64_t)L.plane * es, (cuuint64_t)L.fs * es};
+  cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)bf};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = fn(m, dtype_of<S>(), 4, (void *)base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+    return CGFDM_ERR_CUDA;
+  }
+  return CGFDM_OK;
+}
+
+}  // namespace
+
+template <typename S> bool stage_stream_supported() { return true; }
+template <> bool stage_stream_supported<double>() { return false; }
+
+template <typename S>
+int encode_stream_maps(const S *wave, const S *cjm, const S *wm, const S *t, const Layout &L,
+                       void *out) {
+  static_assert(sizeof(Maps) <= kStreamMapsBytes, "tensor-map buffer too small");
+  Maps m;
+  int rc = encode_map<S>(wave, L, 9, Geo<S>::BX, BY, 9, &m.w);
+  if (!rc) rc = encode_map<S>(cjm, L, 13, TX, TY, 9, &m.c9);
+  if (!rc) rc = encode_map<S>(cjm, L, 13, TX, TY, 3, &m.c3);
+  if (!rc) rc = encode_map<S>(wm, L, 9, TX, TY, 9, &m.m);
+  if (!rc) rc = encode_map<S>(t, L, 9, TX, TY, 9, &m.t);
+  if (!rc) std::memcpy(out, &m, sizeof m);
+  return rc;
+}
+template <>
+int encode_stream_maps<double>(const double *, const double *, const double *, const double *,
+                               const Layout &, void *) {
+  set_error("no streaming kernel for FP64");
+  return CGFDM_ERR_ARG;
+}
+
+template <typename S>
+cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps_in, int *err, int *counter,
+                                cudaStream_t st) {
+  if (a.kend <= a.kbeg) return cudaSuccess;
+  const Maps &m = *(const Maps *)maps_in;
+  const int code = (a.fb1 > 0) * 4 + (a.fb2 > 0) * 2 + (a.fb3 > 0);
+  cudaError_t e;
+  switch (code) {
+    case 0: e = launch_one<S, -1, -1, -1>(a, m, err, counter, st); break;
+    case 1: e = launch_one<S, -1, -1, 1>(a, m, err, counter, st); break;
+    case 2: e = launch_one<S, -1, 1, -1>(a, m, err, counter, st); break;
+    case 3: e = launch_one<S, -1, 1, 1>(a, m, err, counter, st); break;
+    case 4: e = launch_one<S, 1, -1, -1>(a, m, err, counter, st); break;
+    case 5: e = launch_one<S, 1, -1, 1>(a, m, err, counter, st); break;
+    case 6: e = launch_one<S, 1, 1, -1>(a, m, err, counter, st); break;
+    default: e = launch_one<S, 1, 1, 1>(a, m, err, counter, st);
+  }
+  if (e != cudaSuccess || a.nslab == 0) return e;
+  for (int axis = 0; axis < 3; ++axis) {
+    const SlabDev<float> &s0 = a.slab[axis];
+    const int nk = std::min(s0.n2, a.kend - s0.off2);
+    if (nk <= 0) continue;
+    const long long n = (long long)s0.n0 * s0.n1 * nk * (axis == 2 ? 1 : 2);
+    pml_correct_kernel<S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, axis, a.kend);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+template <>
+cudaError_t launch_stage_stream<double>(const StageArgs<double> &, const void *, int *, int *,
+                                        cudaStream_t) {
   return cudaErrorNotSupported;
 }
 
-template bool stage_stream_supported<float>(const StageArgs<float> &);
-template bool stage_stream_supported<__half>(const StageArgs<__half> &);
-template bool stage_stream_supported<__nv_bfloat16>(const StageArgs<__nv_bfloat16> &);
-template bool stage_stream_supported<double>(const StageArgs<double> &);
-template cudaError_t launch_stage_stream<float>(const StageArgs<float> &, cudaStream_t);
-template cudaError_t launch_stage_stream<__half>(const StageArgs<__half> &, cudaStream_t);
-template cudaError_t launch_stage_stream<__nv_bfloat16>(const StageArgs<__nv_bfloat16> &, cudaStream_t);
-template cudaError_t launch_stage_stream<double>(const StageArgs<double> &, cudaStream_t);
+template bool stage_stream_supported<float>();
+template bool stage_stream_supported<__half>();
+template bool stage_stream_supported<__nv_bfloat16>();
+template int encode_stream_maps<float>(const float *, const float *, const float *, const float *,
+                                       const Layout &, void *);
+template int encode_stream_maps<__half>(const __half *, const __half *, const __half *,
+                                        const __half *, const Layout &, void *);
+template int encode_stream_maps<__nv_bfloat16>(const __nv_bfloat16 *, const __nv_bfloat16 *,
+                                               const __nv_bfloat16 *, const __nv_bfloat16 *,
+                                               const Layout &, void *);
+template cudaError_t launch_stage_stream<float>(const StageArgs<float> &, const void *, int *,
+                                                int *, cudaStream_t);
+template cudaError_t launch_stage_stream<__half>(const StageArgs<__half> &, const void *, int *,
+                                                 int *, cudaStream_t);
+template cudaError_t launch_stage_stream<__nv_bfloat16>(const StageArgs<__nv_bfloat16> &,
+                                                        const void *, int *, int *, cudaStream_t);
 
 }  // namespace cgfdm

@@ -108,7 +108,7 @@ def test_run_directory_writes_reference_files(gpu_available, tmp_path, name):
           "layers": g.get("layers"), "source": g.get("source")}
     d = str(tmp_path)
     scenarios.write_inputs(sc, d)
-    cgfdm.run_directory(d)
+    cgfdm.run_directory(d, kernel=cgfdm.KERNEL_EXACT)
     res = scenarios.read_outputs(sc, os.path.join(d, g["params"]["out"]))
     np.testing.assert_array_equal(res["station_xyz"], g["out_station_xyz"])
     np.testing.assert_array_equal(res["station_wave"], g["out_station_wave"])

@@ -1,0 +1,97 @@
+"""The TMA-staged streaming kernel (the fast path) against the reference.
+
+It keeps FMA contraction and forms each direction's elastic combination once
+(scaled by the PML beta and d afterwards), so it agrees with the reference to
+rounding rather than bit for bit.  Tolerances (relative L2 norms):
+  * one RK stage: the stage increment W_out - m within 1e-5 of the
+    reference's increment, per field, and the PML auxiliaries within 1e-5;
+  * complete runs: station seismograms within 1e-5 of the reference's and
+    the PGV map within 1e-5.
+"""
+import numpy as np
+import pytest
+
+import scenarios
+from test_gpu_parity import HALO, _desc, _run_sim, _split_aux_out
+
+pytestmark = pytest.mark.gpu
+cgfdm = pytest.importorskip("cgfdm")
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def stage_golden(gpu_available):
+    return scenarios.load_golden("stage_small.npz")
+
+
+@pytest.mark.parametrize("case", range(len(scenarios.STAGE_CASES)))
+def test_stream_stage_matches_reference(stage_golden, case):
+    g = stage_golden
+    p = g["params"]
+    irk, fb = scenarios.STAGE_CASES[case]
+    with cgfdm.Simulation(_desc(p, 1, kernel=cgfdm.KERNEL_STREAM)) as sim:
+        sim.set_model(g["cjm"], g["rdz"])
+        sim.set_state(irk, W=g["in_W"], t=g["in_t"], m=g["in_m"], aux=g["in_aux"])
+        sim.stage(irk, fb)
+        st = sim.get_state()
+    base = {0: g["in_W"], 1: g["in_m"], 2: g["in_m"], 3: g["in_t"]}[irk]
+    ref = g["case%d_W" % case]
+    for v in range(9):
+        sl = slice(v * ref.size // 9, (v + 1) * ref.size // 9)
+        err = rel_l2(st["W"][sl] - base[sl], ref[sl] - base[sl])
+        assert err < 1e-5, (v, err)
+    ref_aux = _split_aux_out(g["case%d_aux" % case], p)
+    off = 0
+    for n in scenarios.slab_points(p):
+        n9 = 9 * n
+        assert rel_l2(st["aux"][off:off + n9], ref_aux[off:off + n9]) < 1e-5
+        off += 3 * n9
+
+
+@pytest.mark.parametrize("name", ["run_point.npz", "run_fault.npz"])
+def test_stream_full_run_matches_reference(gpu_available, name):
+    g = scenarios.load_golden(name)
+    res = _run_sim(g, kernel=cgfdm.KERNEL_STREAM)
+    for v in range(9):
+        err = rel_l2(res["station_wave"][:, :, v], g["out_station_wave"][:, :, v])
+        assert err < 1e-5, (v, err)
+    assert rel_l2(res["pgv"], g["out_pgv"]) < 1e-5
+    assert rel_l2(res["freesurf"], g["out_freesurf"]) < 1e-5
+
+
+def test_stream_matches_exact_on_larger_grid(gpu_available):
+    """A grid with several tiles in x and y, odd sizes (partial warps and
+    tiles), several z chunks and all PML slabs: the fast path against the
+    exact path (which is bit-identical to the reference), after 20 steps."""
+    nx, ny, nz, npml = 71, 45, 90, 6
+    p = scenarios.S.params(NX=nx, NY=ny, NZ=nz, nPML=npml, DH=100.0, DT=0.008)
+    rng = np.random.default_rng(5)
+    num = (nx + 6) * (ny + 6) * (nz + 6)
+    # a smooth random medium/metric field: perturb a flat-grid CJM
+    cjm = np.zeros((13, nz + 6, ny + 6, nx + 6), np.float32)
+    inner = (slice(None), slice(3, -3), slice(3, -3), slice(3, -3))
+    base = np.array([1, 0, 0, 0, 1, 0, 0, 0, 1, 1e6, 3.2e10, 3.2e10, 1 / 2670.0], np.float32)
+    pert = 1 + 0.05 * rng.standard_normal((13, nz, ny, nx)).astype(np.float32)
+    cjm[inner] = base[:, None, None, None] * pert
+    for f in (1, 2, 3, 5, 6, 7):  # small off-diagonal metrics (a curvilinear grid)
+        cjm[f][inner[1:]] = 0.02 * rng.standard_normal((nz, ny, nx)).astype(np.float32)
+    rdz = (0.1 * rng.standard_normal(18 * (nx + 6) * (ny + 6))).astype(np.float32)
+    sta = np.array([[10, 10, nz + 2], [40, 20, nz + 1], [60, 40, 50]])
+    out = {}
+    for kern in (cgfdm.KERNEL_EXACT, cgfdm.KERNEL_STREAM):
+        with cgfdm.Simulation(_desc(p, 20, kernel=kern)) as sim:
+            sim.set_model(cjm.reshape(-1), rdz)
+            sim.set_point_source(nx // 2, ny // 2, nz // 2, 6.0)
+            sim.set_stations(sta)
+            sim.run(20)
+            out[kern] = (sim.stations(), sim.wavefield(), sim.pgv())
+    e, s = out[cgfdm.KERNEL_EXACT], out[cgfdm.KERNEL_STREAM]
+    assert np.isfinite(s[1]).all()
+    assert rel_l2(s[1], e[1]) < 1e-5
+    for v in range(9):
+        assert rel_l2(s[0][:, :, v], e[0][:, :, v]) < 1e-5
