@@ -225,6 +225,41 @@ def run_reference(w, nsteps, cores, timeout_s=900):
 
 
 # --------------------------------------------------------------------------
+def _propagate(cgfdm, setup, prec, kern, device, nsteps):
+    d0 = setup["desc"]
+    desc = cgfdm.make_desc(d0.nx, d0.ny, d0.nz, d0.npml, d0.dh, d0.dt, nsteps, prec, kern,
+                           device)
+    has_fault = setup["src_index"].size > 0
+    return cgfdm.propagate(
+        desc, setup["cjm"], setup["rdz"], point=setup["point"], rickerfc=setup["rickerfc"],
+        src_index=setup["src_index"] if has_fault else None,
+        moment_rate=setup["moment_rate"] if has_fault else None,
+        src_nt=setup["src_nt"], src_dt=setup["src_dt"], stations=setup["stations"])
+
+
+def measure_accuracy(cgfdm, w, prec, kern, device, nsteps, setup):
+    """Relative L2 error of the seismograms (Vx, Vy, Vz of every station over
+    all steps) and of the final free-surface velocity snapshot, against an
+    FP64 run of the same workload on the GPU."""
+    d = tempfile.mkdtemp(prefix="cgfdm_acc_")
+    try:
+        write_workload(w, d)
+        s64 = cgfdm.setup_from_directory(d, cgfdm.FP64)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    ref = _propagate(cgfdm, s64, cgfdm.FP64, cgfdm.KERNEL_AUTO, device, nsteps)
+    out = _propagate(cgfdm, setup, prec, kern, device, nsteps)
+    rel = lambda a, b: float(np.linalg.norm((a - b).ravel().astype(np.float64)) /
+                             max(np.linalg.norm(b.ravel().astype(np.float64)), 1e-300))
+    nsta = ref[0].shape[0] if ref[0].ndim > 1 else len(setup["stations"])
+    sta_ref = ref[0].reshape(nsta, -1, 9)[:, :nsteps, :3]
+    sta_out = out[0].reshape(nsta, -1, 9)[:, :nsteps, :3]
+    return {"reference": "fp64 GPU run (same workload, same kernels templated on double)",
+            "steps": nsteps, "rel_l2_stations_v": rel(sta_out, sta_ref),
+            "rel_l2_free_surface_v": rel(out[2], ref[2]),
+            "max_abs_ref_v": float(np.abs(sta_ref).max())}
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -244,6 +279,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-steps", type=int, default=20)
+    ap.add_argument("--accuracy-steps", type=int, default=0,
+                    help="also run this many steps in FP64 and in --precision through "
+                         "propagate() and report the relative L2 error of the station "
+                         "seismograms and the free-surface snapshot")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -291,21 +330,17 @@ def main():
             "stream": cgfdm.KERNEL_STREAM}[args.kernel]
 
     total_steps = args.warmup + args.steps
-    w = make_workload(args.workload, max(total_steps, args.e2e_steps) + 2)
+    w = make_workload(args.workload, max(total_steps, args.e2e_steps, args.accuracy_steps) + 2)
     d = tempfile.mkdtemp(prefix="cgfdm_bench_")
     write_workload(w, d)
     t0 = time.perf_counter()
-    setup = cgfdm.setup_from_directory(d)
+    # FP16 / BF16 handles take the coefficients in the reference's scaled form
+    setup = cgfdm.setup_from_directory(d, prec)
     log("host setup %.1f s" % (time.perf_counter() - t0))
     shutil.rmtree(d, ignore_errors=True)
     desc0 = setup["desc"]
     npts = desc0.nx * desc0.ny * desc0.nz
     cjm = setup["cjm"]
-    if prec in (cgfdm.FP16, cgfdm.BF16):
-        # the scaled form needs the scaled coefficients of the FP16 setup
-        d2 = tempfile.mkdtemp(prefix="cgfdm_bench_")
-        write_workload(w, d2)
-        raise SystemExit("reduced-precision bench needs the scaled setup (not wired yet)")
 
     def new_sim(nt):
         desc = cgfdm.make_desc(desc0.nx, desc0.ny, desc0.nz, desc0.npml, desc0.dh, desc0.dt, nt,
@@ -341,6 +376,7 @@ def main():
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     tm = sim.timing_ms()
+    ks = sim.kernel_stats()
     stage_ms, stage_n = float(tm[1]), int(tm[2])
     sim.close()
     ms_t = torch.tensor([ms], device="cuda")
@@ -369,6 +405,10 @@ def main():
         setup["src_index"].nbytes + sta.nbytes
     d2h = out_sta.nbytes + out_pgv.nbytes + out_fs.nbytes
 
+    accuracy = None
+    if args.accuracy_steps > 0:
+        accuracy = measure_accuracy(cgfdm, w, prec, kern, local, args.accuracy_steps, setup)
+
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):
@@ -377,12 +417,22 @@ def main():
     peak_src = "measured" if peak else "fallback"
     peak = peak or 6650.0
     bpp = BYTES_PER_POINT_STEP[args.precision]
-    achieved = npts * bpp / 4.0 * stage_n / (stage_ms / 1e3) / 1e9 if stage_ms > 0 else None
+    # the dominant kernel: the streaming stage kernel (the exact-order kernel
+    # when the precision has no streaming form)
+    if ks["stream_launches"] > 0 and ks["stream_ms"] > 0:
+        kname, kms, klaunch = "stage_stream_kernel", ks["stream_ms"], ks["stream_launches"]
+        kbytes = ks["stream_bytes"]
+    else:
+        kname, kms, klaunch = "stage_exact_kernel", ks["exact_ms"], ks["stages"]
+        kbytes = npts * bpp / 4.0 * ks["stages"]
+    achieved = kbytes / (kms / 1e3) / 1e9 if kms > 0 else None
     traffic = None
     prof = os.path.join(ROOT, "profiles", "stage_traffic.json")
     if os.path.exists(prof):
         try:
-            traffic = json.load(open(prof)).get(args.workload, {}).get(args.precision)
+            t = json.load(open(prof)).get(kname, {}).get(args.precision)
+            if t:  # DRAM bytes of one ncu capture per algorithmic byte, scaled to this launch
+                traffic = t["traffic_over_alg"] * kbytes / max(klaunch, 1)
         except Exception:  # noqa: BLE001
             traffic = None
 
@@ -409,18 +459,28 @@ def main():
                        "grid": [desc0.nx, desc0.ny, desc0.nz], "points": npts,
                        "kernel": args.kernel, "parallelism": "replicas" if ws > 1 else "single",
                        "l2": "inputs larger than L2 (%.2f GB per wavefield buffer), no flush" % (
-                           9 * (desc0.nx + 6) * (desc0.ny + 6) * (desc0.nz + 6) * 4 / 1e9)},
+                           9 * (desc0.nx + 6) * (desc0.ny + 6) * (desc0.nz + 6) *
+                           {"fp32": 4, "fp64": 8}.get(args.precision, 2) / 1e9)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if achieved else None, "traffic": traffic,
-                         "peak_source": peak_src, "bytes_per_point_step": bpp,
-                         "stage_ms_avg": stage_ms / max(stage_n, 1)},
+                         "kernel": kname, "launches": klaunch,
+                         "alg_bytes_per_launch": kbytes / max(klaunch, 1),
+                         "kernel_ms_avg": kms / max(klaunch, 1),
+                         "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)"
+                         if peak_src == "measured" else peak_src,
+                         "bytes_per_point_step": bpp,
+                         "step_share": {"stream": ks["stream_ms"] / ms,
+                                        "pml_correct": ks["pml_correct_ms"] / ms,
+                                        "exact_free_surface": ks["exact_ms"] / ms}},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
                     "d2h_bytes_per_step": d2h / e2e_steps, "steps": e2e_steps,
                     "seconds": float(e2e_t.item())},
-            "gpu_launches": args.steps * (4 + 1 + 1),
+            "gpu_launches": ks["launches"],
             "clocks": clk.summary(),
         }
+        if accuracy:
+            line["accuracy"] = accuracy
         print(json.dumps(line))
     if dist:
         dist.barrier()

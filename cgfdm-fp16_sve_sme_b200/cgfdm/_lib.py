@@ -37,7 +37,8 @@ class Setup(C.Structure):
                 ("point_src", C.c_int32), ("point_xyz", C.c_int32 * 3), ("rickerfc", C.c_float),
                 ("npts", C.c_int64), ("src_nt", C.c_int32), ("src_dt", C.c_float),
                 ("src_index", C.POINTER(C.c_int64)), ("moment_rate", C.POINTER(C.c_float)),
-                ("nsta", C.c_int32), ("sta_xyz", C.POINTER(C.c_int32))]
+                ("nsta", C.c_int32), ("sta_xyz", C.POINTER(C.c_int32)),
+                ("owner", C.c_void_p)]
 
 
 _lib = None
@@ -67,10 +68,12 @@ SIGNATURES = {
     "cgfdm_aux_floats": (C.c_int, [P, C.POINTER(I64)]),
     "cgfdm_set_timing": (C.c_int, [P, I32]),
     "cgfdm_get_timing": (C.c_int, [P, P]),
+    "cgfdm_get_kernel_stats": (C.c_int, [P, P]),
     "cgfdm_propagate": (C.c_int, [C.POINTER(Desc), P, P, I32, P, F, P, P, I64, I32, F, P, I32,
                                   P, P, P]),
     "cgfdm_run_directory": (C.c_int, [C.c_char_p, I32, I32, I32]),
     "cgfdm_setup_from_directory": (C.c_int, [C.c_char_p, C.POINTER(Setup)]),
+    "cgfdm_setup_from_directory_ex": (C.c_int, [C.c_char_p, I32, C.POINTER(Setup)]),
     "cgfdm_free_setup": (C.c_int, [C.POINTER(Setup)]),
 }
 

@@ -108,6 +108,14 @@ class Simulation:
         check(lib().cgfdm_get_timing(self._h, _ptr(ms)))
         return ms
 
+    def kernel_stats(self):
+        """Per-kernel device view of the last run (cgfdm_get_kernel_stats)."""
+        v = np.zeros(8, np.float64)
+        check(lib().cgfdm_get_kernel_stats(self._h, _ptr(v)))
+        return {"stream_ms": v[0], "stream_launches": int(v[1]), "stream_bytes": v[2],
+                "launches": int(v[3]), "pml_correct_ms": v[4], "exact_ms": v[5],
+                "stages": int(v[6])}
+
     # ---- outputs ----------------------------------------------------------
     def stations(self):
         out = np.zeros((self.nsta, self.desc.nt, 9), np.float32)
@@ -168,29 +176,53 @@ def propagate(desc, cjm, rdz, *, point=None, rickerfc=0.0, src_index=None, momen
     return out_sta, out_pgv, out_fs
 
 
-def setup_from_directory(run_dir):
-    """Host setup (params.json, station.json, model files) -> dict of arrays."""
+class _SetupOwner:
+    """Releases a library-built setup once no array views it any more."""
+
+    def __init__(self, s):
+        self.s = s
+
+    def __del__(self):
+        try:
+            lib().cgfdm_free_setup(C.byref(self.s))
+        except Exception:  # noqa: BLE001  (interpreter shutdown)
+            pass
+
+
+def _view(ptr, n, ctype, dtype, owner):
+    if n == 0:
+        return np.zeros(0, dtype)
+    buf = (ctype * n).from_address(C.addressof(ptr.contents))
+    buf._owner = owner  # keeps the library storage alive while viewed
+    return np.frombuffer(buf, dtype=dtype)
+
+
+def setup_from_directory(run_dir, precision=_lib.FP32):
+    """Host setup (params.json, station.json, model files) -> dict of arrays.
+
+    precision selects the storage scaling of cjm and the moment rates
+    (FP16/BF16: the reference's Cv, Cs, Crho).  The arrays are views of the
+    library's own buffers (no copies), released when the last view goes.
+    """
     s = _lib.Setup()
-    check(lib().cgfdm_setup_from_directory(run_dir.encode(), C.byref(s)))
-    try:
-        d = s.desc
-        nx_, ny_, nz_ = d.nx + 6, d.ny + 6, d.nz + 6
-        num, nsurf = nx_ * ny_ * nz_, nx_ * ny_
-        cp = lambda p, n: np.ctypeslib.as_array(p, shape=(n,)).copy() if n else np.zeros(0)
-        out = {
-            "desc": Desc(*[getattr(d, f) for f, _ in Desc._fields_]),
-            "cjm": cp(s.cjm, 13 * num), "rdz": cp(s.rdz, 18 * nsurf),
-            "coord": cp(s.coord, 3 * num), "medium": cp(s.medium, 3 * num),
-            "pml": cp(s.pml, 3 * (nx_ + ny_ + nz_)),
-            "point": tuple(s.point_xyz) if s.point_src else None, "rickerfc": s.rickerfc,
-            "src_index": cp(s.src_index, s.npts), "moment_rate": cp(s.moment_rate,
-                                                                   s.npts * s.src_nt * 6),
-            "src_nt": s.src_nt, "src_dt": s.src_dt,
-            "stations": cp(s.sta_xyz, 3 * s.nsta).reshape(-1, 3),
-        }
-    finally:
-        lib().cgfdm_free_setup(C.byref(s))
-    return out
+    check(lib().cgfdm_setup_from_directory_ex(run_dir.encode(), int(precision), C.byref(s)))
+    owner = _SetupOwner(s)
+    d = s.desc
+    nx_, ny_, nz_ = d.nx + 6, d.ny + 6, d.nz + 6
+    num, nsurf = nx_ * ny_ * nz_, nx_ * ny_
+    f32 = lambda p, n: _view(p, n, C.c_float, np.float32, owner)
+    return {
+        "desc": Desc(*[getattr(d, f) for f, _ in Desc._fields_]),
+        "cjm": f32(s.cjm, 13 * num), "rdz": f32(s.rdz, 18 * nsurf),
+        "coord": f32(s.coord, 3 * num), "medium": f32(s.medium, 3 * num),
+        "pml": f32(s.pml, 3 * (nx_ + ny_ + nz_)),
+        "point": tuple(s.point_xyz) if s.point_src else None, "rickerfc": s.rickerfc,
+        "src_index": _view(s.src_index, s.npts, C.c_int64, np.int64, owner),
+        "moment_rate": f32(s.moment_rate, s.npts * s.src_nt * 6),
+        "src_nt": s.src_nt, "src_dt": s.src_dt,
+        "stations": _view(s.sta_xyz, 3 * s.nsta, C.c_int32, np.int32, owner).reshape(-1, 3),
+        "precision": int(precision),
+    }
 
 
 def run_directory(run_dir, precision=_lib.FP32, kernel=_lib.KERNEL_AUTO, device=0):

@@ -182,6 +182,12 @@ int cgfdm_get_timing(cgfdm_handle *h, float *ms3) {
   return h->eng->get_timing(ms3);
 }
 
+int cgfdm_get_kernel_stats(cgfdm_handle *h, double *out8) {
+  H_OR_FAIL(h);
+  if (!out8) return CGFDM_ERR_ARG;
+  return h->eng->get_kernel_stats(out8);
+}
+
 int cgfdm_propagate(const cgfdm_desc *desc, const float *cjm, const float *rdz, int32_t point_src,
                     const int32_t *point_xyz, float rickerfc, const int64_t *src_index,
                     const float *moment_rate, int64_t npts, int32_t src_nt, float src_dt,
@@ -207,50 +213,43 @@ int cgfdm_propagate(const cgfdm_desc *desc, const float *cjm, const float *rdz, 
   return CGFDM_OK;
 }
 
-int cgfdm_setup_from_directory(const char *run_dir, cgfdm_setup *out) {
+int cgfdm_setup_from_directory_ex(const char *run_dir, int32_t precision, cgfdm_setup *out) {
   if (!run_dir || !out) return CGFDM_ERR_ARG;
+  if (precision < CGFDM_FP32 || precision > CGFDM_FP64) return CGFDM_ERR_ARG;
   return guarded([&] {
     std::memset(out, 0, sizeof *out);
-    cgfdm::Setup s;
-    int rc = cgfdm::build_setup(run_dir, CGFDM_FP32, s);
+    // the arrays stay in the setup's own vectors; `owner` keeps them alive
+    std::unique_ptr<cgfdm::Setup> s(new cgfdm::Setup);
+    int rc = cgfdm::build_setup(run_dir, precision, *s);
     if (rc) return rc;
-    out->desc = s.desc;
-    auto dup = [](const auto &v) {
-      using T = typename std::decay<decltype(v)>::type::value_type;
-      T *p = (T *)std::malloc(sizeof(T) * (v.size() ? v.size() : 1));
-      if (!p) throw std::bad_alloc();
-      if (!v.empty()) std::memcpy(p, v.data(), sizeof(T) * v.size());
-      return p;
-    };
-    out->cjm = dup(s.cjm);
-    out->rdz = dup(s.rdz);
-    out->coord = dup(s.coord);
-    out->medium = dup(s.medium);
-    out->pml = dup(s.pml);
-    out->point_src = s.point_src;
-    std::memcpy(out->point_xyz, s.point_xyz, sizeof s.point_xyz);
-    out->rickerfc = s.p.rickerfc;
-    out->npts = (int64_t)s.src_index.size();
-    out->src_nt = s.src_nt;
-    out->src_dt = s.src_dt;
-    out->src_index = dup(s.src_index);
-    out->moment_rate = dup(s.moment_rate);
-    out->nsta = (int32_t)s.sta_xyz.size() / 3;
-    out->sta_xyz = dup(s.sta_xyz);
+    out->desc = s->desc;
+    out->cjm = s->cjm.data();
+    out->rdz = s->rdz.data();
+    out->coord = s->coord.data();
+    out->medium = s->medium.data();
+    out->pml = s->pml.data();
+    out->point_src = s->point_src;
+    std::memcpy(out->point_xyz, s->point_xyz, sizeof s->point_xyz);
+    out->rickerfc = s->p.rickerfc;
+    out->npts = (int64_t)s->src_index.size();
+    out->src_nt = s->src_nt;
+    out->src_dt = s->src_dt;
+    out->src_index = s->src_index.data();
+    out->moment_rate = s->moment_rate.data();
+    out->nsta = (int32_t)s->sta_xyz.size() / 3;
+    out->sta_xyz = s->sta_xyz.data();
+    out->owner = s.release();
     return CGFDM_OK;
   });
 }
 
+int cgfdm_setup_from_directory(const char *run_dir, cgfdm_setup *out) {
+  return cgfdm_setup_from_directory_ex(run_dir, CGFDM_FP32, out);
+}
+
 int cgfdm_free_setup(cgfdm_setup *s) {
   if (!s) return CGFDM_ERR_ARG;
-  std::free(s->cjm);
-  std::free(s->rdz);
-  std::free(s->coord);
-  std::free(s->medium);
-  std::free(s->pml);
-  std::free(s->src_index);
-  std::free(s->moment_rate);
-  std::free(s->sta_xyz);
+  delete (cgfdm::Setup *)s->owner;
   std::memset(s, 0, sizeof *s);
   return CGFDM_OK;
 }

@@ -241,10 +241,10 @@ template <typename S> class EngineT : public Engine {
       return CGFDM_ERR_ARG;
     }
     last_stream_ = st;
-    if (timing_) {
-      stage_used_ = 0;
-      CUDA_TRY(cudaEventRecord(ev_[0], st));
-    }
+    stage_used_ = 0;
+    launches_ = 0;
+    stream_bytes_ = 0.0;
+    if (timing_) CUDA_TRY(cudaEventRecord(ev_[0], st));
     for (int s = 0; s < nsteps; ++s) {
       const int it = it_;
       // sources add into W once per step before stage 0 (propagate.cpp:145-151)
@@ -254,6 +254,7 @@ template <typename S> class EngineT : public Engine {
         const double CsDT = SCALE_OF<S>::cs * (double)d_.dt;
         CUDA_TRY(launch_point_source<S>(A_, X_, Y_, cjm_, g_.L, psrc_[0], psrc_[1], psrc_[2],
                                         amp343_, sm, DH3, CsDT, st));
+        ++launches_;
       }
       if (fault_on_) {
         // addMoment.cpp:238-264
@@ -265,6 +266,7 @@ template <typename S> class EngineT : public Engine {
           float t1 = float(srcIt) * fdt_;
           float tw = (tmpT - t1) / fdt_;
           CUDA_TRY(launch_fault_source<S>(A_, g_.L.fs, fidx_, frate_, fnpts_, srcIt, tw, d_.dt, st));
+          if (fnpts_ > 0) ++launches_;
         }
       }
       int fb[3] = {kFB[it % 8][0], kFB[it % 8][1], kFB[it % 8][2]};
@@ -276,6 +278,7 @@ template <typename S> class EngineT : public Engine {
       const float c1 = (float)(1.0 / SCALE_OF<S>::cv), c2 = (float)(1.0 / SCALE_OF<S>::cs);
       CUDA_TRY(launch_station_pgv<S>(A_, g_.L, sta_xyz_, nsta_, d_.nt, it, sta_wave_, pgv_, c1, c2,
                                      1.0 / SCALE_OF<S>::cv, st));
+      ++launches_;
       ++it_;
     }
     if (timing_) CUDA_TRY(cudaEventRecord(ev_[1], st));
@@ -420,11 +423,33 @@ template <typename S> class EngineT : public Engine {
     double sum = 0;
     for (int q = 0; q < stage_used_; ++q) {
       float ms = 0;
-      CUDA_TRY(cudaEventElapsedTime(&ms, stage_ev_[2 * q], stage_ev_[2 * q + 1]));
+      CUDA_TRY(cudaEventElapsedTime(&ms, stage_ev_[4 * q], stage_ev_[4 * q + 3]));
       sum += ms;
     }
     ms3[1] = (float)sum;
     ms3[2] = (float)stage_used_;
+    return CGFDM_OK;
+  }
+
+  int get_kernel_stats(double *out) override {
+    int rc = synchronize();
+    if (rc) return rc;
+    for (int q = 0; q < 8; ++q) out[q] = 0.0;
+    out[3] = launches_;
+    if (!timing_) return CGFDM_OK;
+    double part[3] = {0, 0, 0};
+    for (int q = 0; q < stage_used_; ++q)
+      for (int p = 0; p < 3; ++p) {
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, stage_ev_[4 * q + p], stage_ev_[4 * q + p + 1]));
+        part[p] += ms;
+      }
+    out[0] = part[0];
+    out[1] = use_stream_ ? stage_used_ : 0;
+    out[2] = stream_bytes_;
+    out[4] = part[1];
+    out[5] = part[2];
+    out[6] = stage_used_;
     return CGFDM_OK;
   }
 
@@ -473,29 +498,48 @@ template <typename S> class EngineT : public Engine {
     }
     last_out_ = a.wout;
     last_aux_out_ = aux_total_ > 0 ? auxbuf(out_of[irk]) : nullptr;
+    // events per timed stage: [0] start, [1] after the streaming kernel,
+    // [2] after its PML corrections, [3] end (after the exact-order kernel)
+    cudaEvent_t *ev = nullptr;
     if (timing_) {
-      while ((int)stage_ev_.size() < 2 * (stage_used_ + 1)) {
-        cudaEvent_t ev;
-        CUDA_TRY(cudaEventCreate(&ev));
-        stage_ev_.push_back(ev);
+      while ((int)stage_ev_.size() < 4 * (stage_used_ + 1)) {
+        cudaEvent_t e;
+        CUDA_TRY(cudaEventCreate(&e));
+        stage_ev_.push_back(e);
       }
-      CUDA_TRY(cudaEventRecord(stage_ev_[2 * stage_used_], st));
+      ev = &stage_ev_[4 * stage_used_];
+      CUDA_TRY(cudaEventRecord(ev[0], st));
     }
     const int ksurf = g_.L.nz_ - HALO - 3;  // first of the three free-surface layers
     if (use_stream_) {
       StageArgs<S> b = a;
       b.kbeg = HALO;
       b.kend = ksurf;
-      CUDA_TRY(launch_stage_stream<S>(b, tmap_[in_of[irk]], err_flag_, err_flag_ + 1, st));
+      CUDA_TRY(launch_stage_stream<S>(b, tmap_[in_of[irk]], err_flag_, err_flag_ + 1, st,
+                                      ev ? ev[1] : nullptr, &launches_));
+      if (ev) CUDA_TRY(cudaEventRecord(ev[2], st));
+      // fields read and written per point by this stage: W in, 12 coefficients,
+      // W out, plus m (stages 1, 2) and t (written in 0, updated in 1-2, read in 3)
+      static const int nfield[4] = {39, 57, 57, 39};
+      stream_bytes_ += (double)nfield[irk] * sizeof(S) * (double)(g_.nx) * g_.ny * (ksurf - HALO);
       a.kbeg = ksurf;
       a.kend = g_.L.nz_ - HALO;
       CUDA_TRY(launch_stage_exact<S>(a, st));
+      ++launches_;
     } else {
+      if (ev) {
+        CUDA_TRY(cudaEventRecord(ev[1], st));
+        CUDA_TRY(cudaEventRecord(ev[2], st));
+      }
       a.kbeg = HALO;
       a.kend = g_.L.nz_ - HALO;
       CUDA_TRY(launch_stage_exact<S>(a, st));
+      ++launches_;
     }
-    if (timing_) CUDA_TRY(cudaEventRecord(stage_ev_[2 * stage_used_++ + 1], st));
+    if (ev) {
+      CUDA_TRY(cudaEventRecord(ev[3], st));
+      ++stage_used_;
+    }
     return CGFDM_OK;
   }
 
@@ -573,6 +617,8 @@ template <typename S> class EngineT : public Engine {
   cudaEvent_t ev_[2] = {};
   std::vector<cudaEvent_t> stage_ev_;
   int stage_used_ = 0;
+  int launches_ = 0;          // kernels launched by the last run()
+  double stream_bytes_ = 0;   // algorithmic bytes of its streaming-kernel launches
 };
 
 }  // namespace

@@ -23,9 +23,13 @@ template <typename S> cudaError_t launch_stage_exact(const StageArgs<S> &a, cuda
 // below the three free-surface layers.  `maps` holds the tensor maps of the
 // stage input wavefield and of the coefficients (encode_stream_maps).
 constexpr int kStreamMapsBytes = 640;
+// `after_main` (optional) is recorded right after the streaming kernel,
+// before the PML corrections; `nlaunch` (optional) is increased by the
+// number of kernels launched.
 template <typename S>
 cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps, int *err_flag,
-                                int *work_counter, cudaStream_t st);
+                                int *work_counter, cudaStream_t st,
+                                cudaEvent_t after_main = nullptr, int *nlaunch = nullptr);
 template <typename S> bool stage_stream_supported();
 // Encodes the tensor maps the streaming kernel loads its tiles through (the
 // 9 wavefield components of the stage input `wave`, the 13 coefficient

@@ -603,7 +603,7 @@ int encode_stream_maps<double>(const double *, const double *, const double *, c
 
 template <typename S>
 cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps_in, int *err, int *counter,
-                                cudaStream_t st) {
+                                cudaStream_t st, cudaEvent_t after_main, int *nlaunch) {
   if (a.kend <= a.kbeg) return cudaSuccess;
   const Maps &m = *(const Maps *)maps_in;
   const int code = (a.fb1 > 0) * 4 + (a.fb2 > 0) * 2 + (a.fb3 > 0);
@@ -618,7 +618,13 @@ cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps_in, int 
     case 6: e = launch_one<S, 1, 1, -1>(a, m, err, counter, st); break;
     default: e = launch_one<S, 1, 1, 1>(a, m, err, counter, st);
   }
-  if (e != cudaSuccess || a.nslab == 0) return e;
+  if (e != cudaSuccess) return e;
+  if (nlaunch) ++*nlaunch;
+  if (after_main) {
+    e = cudaEventRecord(after_main, st);
+    if (e != cudaSuccess) return e;
+  }
+  if (a.nslab == 0) return cudaSuccess;
   for (int axis = 0; axis < 3; ++axis) {
     const SlabDev<float> &s0 = a.slab[axis];
     const int nk = std::min(s0.n2, a.kend - s0.off2);
@@ -627,12 +633,13 @@ cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps_in, int 
     pml_correct_kernel<S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, axis, a.kend);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (nlaunch) ++*nlaunch;
   }
   return cudaSuccess;
 }
 template <>
 cudaError_t launch_stage_stream<double>(const StageArgs<double> &, const void *, int *, int *,
-                                        cudaStream_t) {
+                                        cudaStream_t, cudaEvent_t, int *) {
   return cudaErrorNotSupported;
 }
 
@@ -647,10 +654,10 @@ template int encode_stream_maps<__nv_bfloat16>(const __nv_bfloat16 *, const __nv
                                                const __nv_bfloat16 *, const __nv_bfloat16 *,
                                                const Layout &, void *);
 template cudaError_t launch_stage_stream<float>(const StageArgs<float> &, const void *, int *,
-                                                int *, cudaStream_t);
+                                                int *, cudaStream_t, cudaEvent_t, int *);
 template cudaError_t launch_stage_stream<__half>(const StageArgs<__half> &, const void *, int *,
-                                                 int *, cudaStream_t);
+                                                 int *, cudaStream_t, cudaEvent_t, int *);
 template cudaError_t launch_stage_stream<__nv_bfloat16>(const StageArgs<__nv_bfloat16> &,
-                                                        const void *, int *, int *, cudaStream_t);
+                                                        const void *, int *, int *, cudaStream_t, cudaEvent_t, int *);
 
 }  // namespace cgfdm

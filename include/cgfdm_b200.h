@@ -12,7 +12,7 @@
  *                  float *momentRate, float *momentRateSlice, SLICE,
  *                  SLICE_DATA, SLICE_DATA)
  *   (src-new-FP32-SVE/functions.h:133-138, propagate.cpp:24-228), called once
- *   from run() (run.cpp:142-146) on every MPI rank.  This library is the
+ *   from run() (run.cpp:100-104) on every MPI rank.  This library is the
  *   single-rank drop-in: no halo exchange, the whole grid on one GPU.
  *
  * Array layouts are the reference's (XFAST, HALO = 3, padded dims
@@ -154,6 +154,14 @@ int cgfdm_aux_floats(cgfdm_handle *h, int64_t *n);   /* floats of one aux set */
 int cgfdm_set_timing(cgfdm_handle *h, int32_t on);
 int cgfdm_get_timing(cgfdm_handle *h, float *ms3);
 
+/* Per-kernel view of the last cgfdm_run (device events, timing enabled):
+ * [0] streaming-kernel time in ms, [1] its launches, [2] the algorithmic
+ * bytes those launches move (fields read and written once per point and
+ * stage), [3] kernels launched by the run (counted whether or not timing is
+ * on), [4] PML-correction time in ms, [5] exact-order (free-surface) kernel
+ * time in ms, [6] stages timed, [7] reserved. */
+int cgfdm_get_kernel_stats(cgfdm_handle *h, double *out8);
+
 /* Drop-in for propagate() with host buffers: uploads the model and sources,
  * runs all nt steps, returns station seismograms, the PGV map and the final
  * free-surface snapshot.  Any output pointer may be NULL. */
@@ -191,9 +199,15 @@ typedef struct {
   float *moment_rate;     /* [src_nt][npts][6], scaled */
   int32_t nsta;
   int32_t *sta_xyz;       /* [nsta][3] padded */
+  void *owner;            /* library-owned storage behind the arrays */
 } cgfdm_setup;
 
+/* FP32 storage constants (cgfdm_setup_from_directory_ex with CGFDM_FP32). */
 int cgfdm_setup_from_directory(const char *run_dir, cgfdm_setup *out);
+/* precision selects the storage scaling of cjm and the moment rates: for
+ * CGFDM_FP16 / CGFDM_BF16 the reference's FP16 constants Cv, Cs, Crho
+ * (macro.h:65-73), the form a handle of that precision expects. */
+int cgfdm_setup_from_directory_ex(const char *run_dir, int32_t precision, cgfdm_setup *out);
 int cgfdm_free_setup(cgfdm_setup *s);
 
 #ifdef __cplusplus
