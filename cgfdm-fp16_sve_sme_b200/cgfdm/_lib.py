@@ -41,6 +41,17 @@ class Setup(C.Structure):
                 ("owner", C.c_void_p)]
 
 
+class StageBuffers(C.Structure):
+    """cgfdm_stage_buffers: device pointers of one no-allocation stage."""
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("npml", C.c_int32),
+                ("dh", C.c_float), ("dt", C.c_float), ("precision", C.c_int32),
+                ("irk", C.c_int32), ("fb1", C.c_int32), ("fb2", C.c_int32), ("fb3", C.c_int32),
+                ("w_in", C.c_void_p), ("w_out", C.c_void_p), ("w_m", C.c_void_p),
+                ("t", C.c_void_p), ("cjm", C.c_void_p), ("rdz", C.c_void_p),
+                ("aux_in", C.c_void_p), ("aux_out", C.c_void_p), ("aux_m", C.c_void_p),
+                ("aux_t", C.c_void_p)]
+
+
 _lib = None
 
 # name -> (restype, argtypes); every entry point returns int unless noted
@@ -75,6 +86,7 @@ SIGNATURES = {
     "cgfdm_setup_from_directory": (C.c_int, [C.c_char_p, C.POINTER(Setup)]),
     "cgfdm_setup_from_directory_ex": (C.c_int, [C.c_char_p, I32, C.POINTER(Setup)]),
     "cgfdm_free_setup": (C.c_int, [C.POINTER(Setup)]),
+    "cgfdm_stage_noalloc": (C.c_int, [C.POINTER(StageBuffers), P, I32]),
 }
 
 

@@ -225,10 +225,30 @@ def setup_from_directory(run_dir, precision=_lib.FP32):
     }
 
 
+def hbm_layout(nx, ny, nz, elem_bytes):
+    """The device layout of wavefield and coefficient buffers (the formula in
+    include/cgfdm_b200.h beside cgfdm_stage_buffers): field f of padded point
+    (i, j, k) at element f * fs + xoff + i + j * px + k * plane."""
+    nx_, ny_, nz_ = nx + 6, ny + 6, nz + 6
+    xoff = 128 // elem_bytes - 3
+    px = (nx_ + xoff + 31) // 32 * 32
+    plane = px * ny_
+    fs = (plane * nz_ + 31) // 32 * 32
+    return {"nx_": nx_, "ny_": ny_, "nz_": nz_, "xoff": xoff, "px": px, "plane": plane,
+            "fs": fs}
+
+
+def stage_noalloc(buffers, stream=None, wait=True):
+    """cgfdm_stage_noalloc: one RK stage on device buffers the caller already
+    owns (a StageBuffers of device pointers), for hosts that cannot allocate
+    device memory while running.  Allocates nothing."""
+    check(lib().cgfdm_stage_noalloc(C.byref(buffers), stream, int(wait)))
+
+
 def run_directory(run_dir, precision=_lib.FP32, kernel=_lib.KERNEL_AUTO, device=0):
     """The reference program on one GPU: reads run_dir, writes its outputs."""
     check(lib().cgfdm_run_directory(run_dir.encode(), precision, kernel, device))
 
 
 __all__ = ["Simulation", "propagate", "setup_from_directory", "run_directory", "make_desc",
-           "device_bytes", "CgfdmError"]
+           "device_bytes", "CgfdmError", "hbm_layout", "stage_noalloc"]

@@ -162,6 +162,61 @@ int cgfdm_get_timing(cgfdm_handle *h, float *ms3);
  * time in ms, [6] stages timed, [7] reserved. */
 int cgfdm_get_kernel_stats(cgfdm_handle *h, double *out8);
 
+/* ---- one RK stage without any device allocation ------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * while they run -- a serving process that splits all of HBM into fixed pools
+ * at start-up, or a framework whose allocator owns every byte of device
+ * memory -- this runs the same stage as cgfdm_stage on a handle (streaming
+ * kernel below the three free-surface layers, exact-order kernel for them)
+ * on buffers the caller already owns, and allocates nothing.  Its only
+ * scratch (error flag, work-queue counter, PML profile table) is a fixed
+ * 64 KiB device array per device, held by every GPU that loads the library.
+ *
+ * Every pointer is DEVICE memory, 256-byte aligned (as cudaMalloc returns).
+ * Wavefields (9 fields: Vx Vy Vz Txx Tyy Tzz Txy Txz Tyz) and cjm (13 fields,
+ * as CJM.cpp) are in the storage type, scaled as a handle of that precision
+ * expects, in the library's device layout for elem_bytes = 4 (FP32) or 2
+ * (FP16 / BF16): _nx_ = nx + 6, _ny_ = ny + 6, _nz_ = nz + 6,
+ * xoff = 128 / elem_bytes - 3, px = roundup(_nx_ + xoff, 32),
+ * plane = px * _ny_, fs = roundup(plane * _nz_, 32); field f of padded point
+ * (i, j, k) at element f * fs + xoff + i + j * px + k * plane.  rdz is
+ * 2 x (_nx_*_ny_) x 9 float.  The four auxiliary buffers are float, each the
+ * slabs x1 y1 z1 x2 y2 concatenated ([pos][9], pos x-fastest), as many floats
+ * as cgfdm_aux_floats reports for a handle of the same grid.  Stage irk reads
+ * w_in, cjm, rdz, w_m (stages 1-2), t (stages 1-3), aux_in, aux_m (stages
+ * 1-2), aux_t (stages 1-3), and writes w_out, t (stages 0-2), aux_out and
+ * aux_t (stages 0-2).
+ *
+ * Limits and rules: precision FP32, FP16 or BF16; the PML profile table must
+ * fit the scratch (nx + ny + nz + 18 <= 5440, else CGFDM_ERR_ARG).  All calls
+ * on one device share the scratch and see what the last call left there:
+ * each call zeroes the work-queue counter itself, so calls whose work
+ * overlaps on the GPU race.  The error flag starts at zero, is set by an
+ * expired bounded wait, and is read and cleared only when `wait` is
+ * non-zero: then the call synchronizes `stream` and returns CGFDM_ERR_TIMEOUT
+ * if it was set.  With wait = 0 the call only enqueues work on `stream`
+ * (current device).  The first call on a device resolves the scratch address
+ * and kernel attributes; make it before any stream capture.
+ */
+typedef struct {
+  int32_t nx, ny, nz, npml;
+  float dh, dt;
+  int32_t precision;
+  int32_t irk, fb1, fb2, fb3;
+  const void *w_in;
+  void *w_out;
+  const void *w_m;
+  void *t;
+  const void *cjm;
+  const float *rdz;
+  const float *aux_in;
+  float *aux_out;
+  const float *aux_m;
+  float *aux_t;
+} cgfdm_stage_buffers;
+
+int cgfdm_stage_noalloc(const cgfdm_stage_buffers *b, void *stream, int32_t wait);
+
 /* Drop-in for propagate() with host buffers: uploads the model and sources,
  * runs all nt steps, returns station seismograms, the PGV map and the final
  * free-surface snapshot.  Any output pointer may be NULL. */
