@@ -470,7 +470,6 @@ def main():
                          if peak_src == "measured" else peak_src,
                          "bytes_per_point_step": bpp,
                          "step_share": {"stream": ks["stream_ms"] / ms,
-                                        "pml_correct": ks["pml_correct_ms"] / ms,
                                         "exact_free_surface": ks["exact_ms"] / ms}},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,

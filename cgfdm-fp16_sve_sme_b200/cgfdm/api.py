@@ -113,7 +113,7 @@ class Simulation:
         v = np.zeros(8, np.float64)
         check(lib().cgfdm_get_kernel_stats(self._h, _ptr(v)))
         return {"stream_ms": v[0], "stream_launches": int(v[1]), "stream_bytes": v[2],
-                "launches": int(v[3]), "pml_correct_ms": v[4], "exact_ms": v[5],
+                "launches": int(v[3]), "gap_ms": v[4], "exact_ms": v[5],
                 "stages": int(v[6])}
 
     # ---- outputs ----------------------------------------------------------

@@ -499,7 +499,7 @@ template <typename S> class EngineT : public Engine {
     last_out_ = a.wout;
     last_aux_out_ = aux_total_ > 0 ? auxbuf(out_of[irk]) : nullptr;
     // events per timed stage: [0] start, [1] after the streaming kernel,
-    // [2] after its PML corrections, [3] end (after the exact-order kernel)
+    // [2] before the exact-order kernel, [3] end (after the exact-order kernel)
     cudaEvent_t *ev = nullptr;
     if (timing_) {
       while ((int)stage_ev_.size() < 4 * (stage_used_ + 1)) {

@@ -24,7 +24,7 @@ template <typename S> cudaError_t launch_stage_exact(const StageArgs<S> &a, cuda
 // stage input wavefield and of the coefficients (encode_stream_maps).
 constexpr int kStreamMapsBytes = 640;
 // `after_main` (optional) is recorded right after the streaming kernel,
-// before the PML corrections; `nlaunch` (optional) is increased by the
+// before the exact-order kernel; `nlaunch` (optional) is increased by the
 // number of kernels launched.
 template <typename S>
 cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps, int *err_flag,

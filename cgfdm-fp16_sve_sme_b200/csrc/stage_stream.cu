@@ -15,7 +15,9 @@
 //   M ring (2): the RK step state m and accumulator t of one output plane
 //               (stages that read them).
 // Every operand of the stage therefore arrives asynchronously ahead of use;
-// only the PML auxiliaries (a minority of points) are read with plain loads.
+// only the PML auxiliaries (a minority of points) are read with plain loads,
+// by a second instantiation (PMLK) that runs the tiles and bottom chunks
+// touching a PML slab.
 // Derivative, elastic combination, PML ADE update and the RK4 combination of
 // wavefield and auxiliaries are fused: each field is read and written once
 // per stage, stores are whole 128-byte lines per warp row.
@@ -60,7 +62,12 @@ template <typename S> struct Geo {
   static constexpr int OFF_C = NW * W_BYTES;
   static constexpr int OFF_M = OFF_C + NC * C_BYTES;
   static constexpr int OFF_BAR = OFF_M + NM * M_BYTES;
+  // PML variant: one 32 x 9 float staging buffer per warp
+  static constexpr int OFF_P = (OFF_BAR + 8 * (NW + NC + NM) + 127) / 128 * 128;
+  static constexpr int P_BYTES = (NTHR / 32) * 32 * 9 * 4;
   static constexpr int SMEM = OFF_BAR + 8 * (NW + NC + NM) + 128;
+  static constexpr int SMEM_P = OFF_P + P_BYTES + 128;
+  static_assert(SMEM_P <= 232448, "shared memory budget");
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -118,41 +125,114 @@ __device__ __forceinline__ void elastic9(const float m[3], const float L[9], flo
   E[8] = (m[2] * L[1] + m[1] * L[2]) * mu;
 }
 
-// PML auxiliary update of one slab point (pml_deriv.cpp:199-237, pml_rk.cpp)
-// given the direction's elastic combination E; adds -beta*Aux*DT into hc.
-__device__ __forceinline__ void pml_point(const SlabDev<float> &sl, long long pos, const float E[9],
-                                          float dl, float ad, float bt, float DT, int irk,
-                                          float hc[9]) {
-  const float *ain = sl.ain + pos * 9;
-  float *aout = sl.aout + pos * 9;
-  float *at = sl.at + pos * 9;
-  const float *am = sl.am + pos * 9;
-#pragma unroll
-  for (int v = 0; v < 9; ++v) {
-    const float a = ain[v];
-    const float ha = (dl * E[v] - ad * a) * DT;
-    hc[v] -= bt * a * DT;
-    switch (irk) {
-      case 0:
-        at[v] = a + kB1 * ha;
-        aout[v] = a + kA2rk * ha;
-        break;
-      case 1:
-        at[v] = at[v] + kB2 * ha;
-        aout[v] = am[v] + kA3rk * ha;
-        break;
-      case 2:
-        at[v] = at[v] + kB3 * ha;
-        aout[v] = am[v] + ha;
-        break;
-      default:
-        aout[v] = at[v] + kB4 * ha;
-    }
-  }
-}
-
 __device__ __forceinline__ long long slab_pos(const SlabDev<float> &sl, int i, int j, int k) {
   return (i - sl.off0) + (long long)(j - sl.off1) * sl.n0 + (long long)(k - sl.off2) * sl.n0 * sl.n1;
+}
+
+// PML of one derivative direction for the lanes of a warp that lie in slab
+// `sid` (pml_deriv.cpp:199-237 and pml_rk.cpp:15-69).  Those lanes are
+// consecutive in x, so their auxiliary records ([pos][9], pos x-fastest)
+// form one contiguous run: the warp reads and writes the run flat (lane l
+// takes elements l, l + 32, ...), fully coalesced, with each owner's elastic
+// combination E staged through the warp's buffer `buf` (32 x 9 floats).  The
+// -beta * Aux * DT term comes back through the same buffer into h.
+// prof: alpha, beta, d of the axis (nax each); the profile index is
+// lbase + lstep * (point within the run).
+// L2 prefetch (a hint) of the 16-byte-aligned part of n floats at p; the run
+// is rounded inward, so nothing outside it is touched.
+__device__ __forceinline__ void prefetch_run(const float *p, int n) {
+  const unsigned long long b = ((unsigned long long)p + 15) & ~15ull;
+  const unsigned long long e = (unsigned long long)(p + n) & ~15ull;
+  if (e > b)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b), "r"((unsigned)(e - b))
+                 : "memory");
+}
+
+__device__ __forceinline__ void pml_warp(unsigned vm, const SlabDev<float> &sl, bool mine,
+                                         long long pos, const float E[9], float h[9], float *buf,
+                                         const float *prof, int nax, int lidx, int lstep,
+                                         int irk, float DT, long long next) {
+  // next: offset in records of the same run one output plane further in the
+  // sweep (0: the item has no further plane); it is prefetched into L2
+  // vm: the lanes of this warp that take part (the valid points of the row)
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned m = __ballot_sync(vm, mine);
+  if (!m) return;
+  const int l0 = __ffs(m) - 1, nact = __popc(m);
+  const long long pos0 = __shfl_sync(vm, pos, l0);
+  const int lbase = __shfl_sync(vm, lidx, l0);
+  if (mine) {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) buf[(lane - l0) * 9 + v] = E[v];
+  }
+  __syncwarp(vm);
+  const int n = nact * 9;
+  const float *__restrict__ ain = sl.ain + pos0 * 9;
+  const float *__restrict__ am = sl.am + pos0 * 9;
+  float *__restrict__ aout = sl.aout + pos0 * 9;
+  float *__restrict__ at = sl.at + pos0 * 9;
+  // the participating lanes (nv of them, this one of rank r) cover the run
+  // flat: element f = f0 + r + nv * q, 9 per lane per batch (one batch when
+  // the whole warp takes part)
+  const int nv = __popc(vm), r = __popc(vm & ((1u << lane) - 1u));
+  if (next && r == 0) {
+    const long long pn = (pos0 + next) * 9;
+    prefetch_run(sl.ain + pn, n);
+    if (irk == 1 || irk == 2) prefetch_run(sl.am + pn, n);
+    if (irk >= 1) prefetch_run(sl.at + pn, n);
+  }
+  for (int f0 = 0; f0 < n; f0 += 9 * nv) {
+    // every load of the batch first: the auxiliary input, and what the stage
+    // adds its increment to (m in stages 1-2, t in stage 3) plus t (stages 1-2)
+    float av[9], bv[9], tv[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const int f = f0 + r + nv * q;
+      av[q] = bv[q] = tv[q] = 0.0f;
+      if (f < n) {
+        av[q] = ain[f];
+        if (irk == 1 || irk == 2) {
+          bv[q] = am[f];
+          tv[q] = at[f];
+        } else if (irk == 3) {
+          bv[q] = at[f];
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const int f = f0 + r + nv * q;
+      if (f < n) {
+        const int l = lbase + lstep * (f / 9);
+        const float dl = prof[2 * nax + l], bt = prof[nax + l], ad = prof[l] + dl;
+        const float a = av[q];
+        const float ha = (dl * buf[f] - ad * a) * DT;
+        buf[f] = -bt * a * DT;
+        switch (irk) {
+          case 0:
+            at[f] = a + kB1 * ha;
+            aout[f] = a + kA2rk * ha;
+            break;
+          case 1:
+            at[f] = tv[q] + kB2 * ha;
+            aout[f] = bv[q] + kA3rk * ha;
+            break;
+          case 2:
+            at[f] = tv[q] + kB3 * ha;
+            aout[f] = bv[q] + ha;
+            break;
+          default:
+            aout[f] = bv[q] + kB4 * ha;
+        }
+      }
+    }
+  }
+  __syncwarp(vm);
+  if (mine) {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) h[v] += buf[(lane - l0) * 9 + v];
+  }
+  __syncwarp(vm);
 }
 
 struct Maps {
@@ -163,12 +243,70 @@ struct Maps {
   CUtensorMap t;   // RK accumulator, box 32 x 16 x 1 x 9
 };
 
+// Work items of one launch.  The z range [kbeg, kend) is cut at kz, the top
+// of the bottom PML slab: nzc chunks of chunk_p planes below it and nic
+// chunks of chunk_i planes above it.  Tiles are 32 x 16 columns on an
+// ntx x nty grid; tiles [bx_lo, bx_hi) x [by_lo, by_hi) touch no x or y PML
+// slab.  The interior launch covers interior tiles x upper chunks; the PML
+// launch covers every tile of the lower chunks and the edge tiles (all
+// others) of the upper chunks.  Tiles vary fastest, so the items running at
+// one time are neighbours at the same depth.
 struct Work {
-  int ntx, nty, nchunk, chunk, nitems;
+  int ntx, nty, bx_lo, bx_hi, by_lo, by_hi;
+  int kz, nzc, chunk_p, nic, chunk_i;
+  int nitems;
   int *counter;
 };
 
-template <typename S, int FB1, int FB2, int FB3>
+template <bool PMLK>
+__device__ __forceinline__ void item_of(const Work &w, int item, int &bxi, int &byi, int &kb,
+                                        int &ke, int kbeg, int kend) {
+  int chk;
+  if (!PMLK) {
+    const int nxi = w.bx_hi - w.bx_lo, ti = nxi * (w.by_hi - w.by_lo);
+    const int t = item % ti;
+    chk = w.nzc + item / ti;
+    bxi = w.bx_lo + t % nxi;
+    byi = w.by_lo + t / nxi;
+  } else {
+    const int tall = w.ntx * w.nty;
+    if (item < w.nzc * tall) {
+      chk = item / tall;
+      bxi = (item % tall) % w.ntx;
+      byi = (item % tall) / w.ntx;
+    } else {
+      const int nside = w.bx_lo + (w.ntx - w.bx_hi);
+      const int nedge = tall - (w.bx_hi - w.bx_lo) * (w.by_hi - w.by_lo);
+      const int q = item - w.nzc * tall;
+      chk = w.nzc + q / nedge;
+      int e = q % nedge;
+      if (e < w.by_lo * w.ntx) {
+        byi = e / w.ntx;
+        bxi = e % w.ntx;
+      } else {
+        e -= w.by_lo * w.ntx;
+        if (e < (w.by_hi - w.by_lo) * nside) {
+          byi = w.by_lo + e / nside;
+          const int r = e % nside;
+          bxi = r < w.bx_lo ? r : w.bx_hi + (r - w.bx_lo);
+        } else {
+          e -= (w.by_hi - w.by_lo) * nside;
+          byi = w.by_hi + e / w.ntx;
+          bxi = e % w.ntx;
+        }
+      }
+    }
+  }
+  if (chk < w.nzc) {
+    kb = kbeg + chk * w.chunk_p;
+    ke = min(kb + w.chunk_p, w.kz);
+  } else {
+    kb = w.kz + (chk - w.nzc) * w.chunk_i;
+    ke = min(kb + w.chunk_i, kend);
+  }
+}
+
+template <typename S, int FB1, int FB2, int FB3, bool PMLK>
 __global__ void __launch_bounds__(NTHR, 1)
     stage_stream_kernel(const __grid_constant__ Maps maps, const StageArgs<S> a, const Work wk,
                         int *err) {
@@ -212,10 +350,8 @@ __global__ void __launch_bounds__(NTHR, 1)
     __syncthreads();
     const int item = s_item;
     if (item >= wk.nitems || s_bad) break;
-    const int tile = item % (wk.ntx * wk.nty), chk = item / (wk.ntx * wk.nty);
-    const int bxi = tile % wk.ntx, byi = tile / wk.ntx;
-    const int kb = a.kbeg + chk * wk.chunk;
-    const int ke = min(kb + wk.chunk, a.kend);
+    int bxi, byi, kb, ke;
+    item_of<PMLK>(wk, item, bxi, byi, kb, ke, a.kbeg, a.kend);
     const int nout = ke - kb, nplanes = nout + 4;
     const int q0 = DIR > 0 ? kb - 3 : ke + 2;  // input planes q_n = q0 + n*DIR
     const int i = HALO + bxi * TX + c, j = HALO + byi * TY + r;
@@ -257,9 +393,19 @@ __global__ void __launch_bounds__(NTHR, 1)
         for (int o = 0; o < NM && o < nout; ++o) issue_m(o);
     }
 
-    // per-column PML beta times DT (the auxiliaries are updated by pml_correct_kernel)
+    // per-column PML beta times DT
     const int ic = valid ? i : HALO, jc = valid ? j : HALO;
     const float bxd = px[L.nx_ + ic] * DT, byd = py[L.ny_ + jc] * DT;
+    // PML variant: the x (x1/x2) and y (y1/y2) slab of this column, and the
+    // valid lanes of this warp row (member mask of the warp-wide PML steps)
+    int sx = -1, sy = -1;
+    if (PMLK && valid && a.nslab) {
+      const int np = a.npml;
+      sx = i < HALO + np ? 0 : i >= L.nx_ - HALO - np ? 3 : -1;
+      sy = j < HALO + np ? 1 : j >= L.ny_ - HALO - np ? 4 : -1;
+    }
+    const unsigned vmask = PMLK ? __ballot_sync(0xffffffffu, valid) : 0u;
+    float *pbuf = PMLK ? (float *)(smem + G::OFF_P) + (tid / 32) * 32 * 9 : nullptr;
 
     // z window in registers: physical slot n mod 5 holds input plane q_n; the
     // plane loop is unrolled five times so that every slot index is a
@@ -303,6 +449,7 @@ __global__ void __launch_bounds__(NTHR, 1)
         const float mu = ldv(cf + 9 * NTHR + cidx), lam = ldv(cf + 10 * NTHR + cidx);
         const float bu = ldv(cf + 11 * NTHR + cidx) * (float)CRHO_OF<S>::v;
         const float bzd = pz[L.nz_ + k] * DT;
+        const bool more = o + 1 < nout;  // this item has a further output plane
         float h[9], Lr[9], E[9];
         // x direction
 #pragma unroll
@@ -314,6 +461,12 @@ __global__ void __launch_bounds__(NTHR, 1)
         elastic9(mx, Lr, mu, lam, bu, E);
 #pragma unroll
         for (int v = 0; v < 9; ++v) h[v] = bxd * E[v];
+        if (PMLK && a.nslab) {
+          pml_warp(vmask, a.slab[0], sx == 0, slab_pos(a.slab[0], i, j, k), E, h, pbuf, px,
+                   L.nx_, i, 1, irk, DT, more ? DIR * (long long)a.slab[0].n0 * a.slab[0].n1 : 0);
+          pml_warp(vmask, a.slab[3], sx == 3, slab_pos(a.slab[3], i, j, k), E, h, pbuf, px,
+                   L.nx_, i, 1, irk, DT, more ? DIR * (long long)a.slab[3].n0 * a.slab[3].n1 : 0);
+        }
         // y direction
 #pragma unroll
         for (int v = 0; v < 9; ++v) {
@@ -324,6 +477,12 @@ __global__ void __launch_bounds__(NTHR, 1)
         elastic9(my, Lr, mu, lam, bu, E);
 #pragma unroll
         for (int v = 0; v < 9; ++v) h[v] += byd * E[v];
+        if (PMLK && a.nslab) {
+          pml_warp(vmask, a.slab[1], sy == 1, slab_pos(a.slab[1], i, j, k), E, h, pbuf, py,
+                   L.ny_, j, 0, irk, DT, more ? DIR * (long long)a.slab[1].n0 * a.slab[1].n1 : 0);
+          pml_warp(vmask, a.slab[4], sy == 4, slab_pos(a.slab[4], i, j, k), E, h, pbuf, py,
+                   L.ny_, j, 0, irk, DT, more ? DIR * (long long)a.slab[4].n0 * a.slab[4].n1 : 0);
+        }
         // z direction: W[k - m*DIR] for m = -1..3 sits in slots P0 (q = k + DIR) .. P4
 #pragma unroll
         for (int v = 0; v < 9; ++v)
@@ -332,6 +491,9 @@ __global__ void __launch_bounds__(NTHR, 1)
         elastic9(mz, Lr, mu, lam, bu, E);
 #pragma unroll
         for (int v = 0; v < 9; ++v) h[v] += bzd * E[v];
+        if (PMLK && a.nslab && k < HALO + a.npml)
+          pml_warp(vmask, a.slab[2], true, slab_pos(a.slab[2], i, j, k), E, h, pbuf, pz, L.nz_,
+                   k, 0, irk, DT, more ? DIR * (long long)a.slab[2].n0 * a.slab[2].n1 : 0);
         // RK4 combination (wave_rk.cpp:13-99)
         const S *ms = (const S *)(smem + G::OFF_M + ((fm0 + o) % NM) * G::M_BYTES);
         const S *ts = ms + 9 * NTHR;
@@ -368,6 +530,20 @@ __global__ void __launch_bounds__(NTHR, 1)
       return true;
     };
     int n = 0;
+    if (PMLK) {
+      // one loop body (small code): the window moves down one slot per plane
+#pragma unroll 1
+      for (; n < nplanes; ++n) {
+        if (!iter(std::integral_constant<int, 0>{}, n)) break;
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+          win[v][1] = win[v][2];
+          win[v][2] = win[v][3];
+          win[v][3] = win[v][4];
+          win[v][4] = win[v][0];
+        }
+      }
+    } else
     while (n < nplanes) {
       if (!iter(std::integral_constant<int, 0>{}, n)) break;
       if (++n >= nplanes) break;
@@ -400,135 +576,81 @@ __global__ void __launch_bounds__(NTHR, 1)
   }
 }
 
-// PML of the streaming path, applied after the streaming kernel to the slab
-// points below the free-surface layers (pml_deriv.cpp:90-544, pml_rk.cpp).
-// For each point of the slabs of one axis: the raw derivative of the stage
-// input along that axis, its elastic combination E, the ADE update of the
-// auxiliaries and their RK4 step, and the -beta*Aux*DT correction added to
-// the already written stage outputs (the RK4 combination is linear in h:
-// wout += a_irk * corr, t += b_irk * corr).  x and y have two disjoint slabs
-// each; launches per axis run in sequence, so points in several slabs
-// (edges, corners) receive the corrections one after the other.
-template <typename S>
-__global__ void __launch_bounds__(256) pml_correct_kernel(const StageArgs<S> a, int axis, int kend) {
-  const Layout L = a.L;
-  const int nsl = axis == 2 ? 1 : 2;
-  const SlabDev<float> &s0 = a.slab[axis];
-  const long long per = (long long)s0.n0 * s0.n1 * (kend - s0.off2 < s0.n2 ? kend - s0.off2 : s0.n2);
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (per <= 0 || t >= per * nsl) return;
-  const int which = (int)(t / per);
-  const SlabDev<float> &sl = a.slab[axis + 3 * which];
-  const long long p = t % per;
-  const int i0 = (int)(p % sl.n0), j0 = (int)((p / sl.n0) % sl.n1), k0 = (int)(p / ((long long)sl.n0 * sl.n1));
-  const int i = sl.off0 + i0, j = sl.off1 + j0, k = sl.off2 + k0;
-  if (k >= kend) return;
-  const long long pos = i0 + (long long)j0 * sl.n0 + (long long)k0 * sl.n0 * sl.n1;
-  const long long fs = L.fs, c = L.at(i, j, k);
-  const long long o = axis == 0 ? 1 : axis == 1 ? L.px : L.plane;
-  const int fb = axis == 0 ? a.fb1 : axis == 1 ? a.fb2 : a.fb3;
-  const int irk = a.irk;
-  const float w0 = fb * kAm1 * a.rDH, w1 = fb * kA0 * a.rDH, w2 = fb * kA1 * a.rDH,
-              w3 = fb * kA2 * a.rDH, w4 = fb * kA3 * a.rDH;
-  const long long q = fb * o;
-  // every load first (the outputs and auxiliaries are rewritten below)
-  const float *__restrict__ ain = sl.ain + pos * 9;
-  const float *__restrict__ am = sl.am + pos * 9;
-  float *__restrict__ aout = sl.aout + pos * 9;
-  float *__restrict__ at = sl.at + pos * 9;
-  S *__restrict__ wo = a.wout + c;
-  S *__restrict__ tw = a.t + c;
-  float av[9], amv[9], atv[9], wov[9], twv[9], Lr[9];
-#pragma unroll
-  for (int v = 0; v < 9; ++v) {
-    av[v] = ain[v];
-    amv[v] = (irk == 1 || irk == 2) ? am[v] : 0.0f;
-    atv[v] = irk >= 1 ? at[v] : 0.0f;
-    wov[v] = ldv(wo + v * fs);
-    twv[v] = irk < 3 ? (float)ldv(tw + v * fs) : 0.0f;
-    const S *w = a.win + v * fs + c;
-    Lr[v] = w0 * ldv(w - q) + w1 * ldv(w) + w2 * ldv(w + q) + w3 * ldv(w + 2 * q) + w4 * ldv(w + 3 * q);
-  }
-  float m[3], E[9];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) m[d] = ldv(a.cjm + c + (3 * axis + d) * fs);
-  const float mu = ldv(a.cjm + c + 10 * fs), lam = ldv(a.cjm + c + 11 * fs);
-  const float bu = ldv(a.cjm + c + 12 * fs) * (float)CRHO_OF<S>::v;
-  elastic9(m, Lr, mu, lam, bu, E);
-  const float *prof = a.pml + (axis == 0 ? 0 : axis == 1 ? 3 * L.nx_ : 3 * (L.nx_ + L.ny_));
-  const int nax = axis == 0 ? L.nx_ : axis == 1 ? L.ny_ : L.nz_;
-  const int l = axis == 0 ? i : axis == 1 ? j : k;
-  const float dl = prof[2 * nax + l], bt = prof[nax + l], ad = prof[l] + dl;
-  const float DT = a.DT;
-  float ca, cb;
-  switch (irk) {
-    case 0: ca = kA2rk; cb = kB1; break;
-    case 1: ca = kA3rk; cb = kB2; break;
-    case 2: ca = 1.0f; cb = kB3; break;
-    default: ca = kB4; cb = 0.0f;
-  }
-#pragma unroll
-  for (int v = 0; v < 9; ++v) {
-    const float x = av[v];
-    const float ha = (dl * E[v] - ad * x) * DT;  // pml_deriv.cpp:199-207
-    const float corr = -bt * x * DT;             // pml_deriv.cpp:219-227
-    switch (irk) {                               // pml_rk.cpp:15-69
-      case 0:
-        at[v] = x + kB1 * ha;
-        aout[v] = x + kA2rk * ha;
-        break;
-      case 1:
-        at[v] = atv[v] + kB2 * ha;
-        aout[v] = amv[v] + kA3rk * ha;
-        break;
-      case 2:
-        at[v] = atv[v] + kB3 * ha;
-        aout[v] = amv[v] + ha;
-        break;
-      default:
-        aout[v] = atv[v] + kB4 * ha;
-    }
-    stv(wo + v * fs, wov[v] + ca * corr);
-    if (irk < 3) stv(tw + v * fs, twv[v] + cb * corr);
-  }
-}
-
-template <typename S, int FB1, int FB2, int FB3>
-cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *counter,
-                       cudaStream_t st) {
+template <typename S, int FB1, int FB2, int FB3, bool PMLK>
+cudaError_t launch_variant(const StageArgs<S> &a, const Maps &maps, const Work &wk, int *err,
+                           int nsm, cudaStream_t st) {
   static int attr_dev = -1;
-  auto kern = stage_stream_kernel<S, FB1, FB2, FB3>;
+  auto kern = stage_stream_kernel<S, FB1, FB2, FB3, PMLK>;
+  const int smem = PMLK ? Geo<S>::SMEM_P : Geo<S>::SMEM;
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
     cudaError_t e =
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Geo<S>::SMEM);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     attr_dev = dev;
   }
+  cudaError_t e = cudaMemsetAsync(wk.counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  kern<<<std::min(wk.nitems, nsm), NTHR, smem, st>>>(maps, a, wk, err);
+  return cudaGetLastError();
+}
+
+// Splits the stage into the interior launch (tiles and chunks that touch no
+// PML slab) and the PML launch (the rest), see Work.
+template <typename S, int FB1, int FB2, int FB3>
+cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *counter,
+                       cudaStream_t st, int *nlaunch) {
   static int nsm = 0;
   if (!nsm) {
+    int dev = 0;
+    cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (nsm <= 0) nsm = 148;
   }
   const int nx = a.L.nx_ - 2 * HALO, ny = a.L.ny_ - 2 * HALO;
+  const int np = a.nslab ? a.npml : 0;
   Work wk;
+  wk.counter = counter;
   wk.ntx = (nx + TX - 1) / TX;
   wk.nty = (ny + TY - 1) / TY;
+  if (np > 0) {
+    wk.bx_lo = (np + TX - 1) / TX;
+    wk.bx_hi = (nx - np) / TX;
+    wk.by_lo = (np + TY - 1) / TY;
+    wk.by_hi = (ny - np) / TY;
+    if (wk.bx_hi <= wk.bx_lo || wk.by_hi <= wk.by_lo) wk.bx_lo = wk.bx_hi = wk.by_lo = wk.by_hi = 0;
+  } else {
+    wk.bx_lo = 0; wk.bx_hi = wk.ntx; wk.by_lo = 0; wk.by_hi = wk.nty;
+  }
   const int tiles = wk.ntx * wk.nty;
-  const int planes = a.kend - a.kbeg;
-  // about 24 items per SM, chunks of at least 24 planes
-  int nchunk = (24 * nsm + tiles - 1) / tiles;
-  nchunk = std::max(1, std::min(nchunk, planes / 24));
-  wk.chunk = (planes + nchunk - 1) / nchunk;
-  wk.nchunk = (planes + wk.chunk - 1) / wk.chunk;
-  wk.nitems = tiles * wk.nchunk;
-  wk.counter = counter;
-  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
-  if (e != cudaSuccess) return e;
-  const int grid = std::min(wk.nitems, nsm);
-  kern<<<grid, NTHR, Geo<S>::SMEM, st>>>(maps, a, wk, err);
-  return cudaGetLastError();
+  const int tiles_in = (wk.bx_hi - wk.bx_lo) * (wk.by_hi - wk.by_lo);
+  // bottom PML planes [kbeg, kz), at most 32 planes per chunk
+  wk.kz = std::min(a.kbeg + np, a.kend);
+  const int pl_p = wk.kz - a.kbeg, pl_i = a.kend - wk.kz;
+  wk.nzc = pl_p > 0 ? (pl_p + 31) / 32 : 0;
+  wk.chunk_p = wk.nzc ? (pl_p + wk.nzc - 1) / wk.nzc : 1;
+  // upper planes: about 24 items per SM, chunks of at least 24 planes
+  int nic = pl_i > 0 ? (24 * nsm + tiles - 1) / tiles : 0;
+  if (pl_i > 0) nic = std::max(1, std::min(nic, pl_i / 24));
+  wk.chunk_i = nic ? (pl_i + nic - 1) / nic : 1;
+  wk.nic = nic ? (pl_i + wk.chunk_i - 1) / wk.chunk_i : 0;
+  cudaError_t e = cudaSuccess;
+  Work wi = wk;
+  wi.nitems = tiles_in * wk.nic;
+  if (wi.nitems > 0) {
+    e = launch_variant<S, FB1, FB2, FB3, false>(a, maps, wi, err, nsm, st);
+    if (e != cudaSuccess) return e;
+    if (nlaunch) ++*nlaunch;
+  }
+  Work wp = wk;
+  wp.nitems = wk.nzc * tiles + (tiles - tiles_in) * wk.nic;
+  if (wp.nitems > 0) {
+    e = launch_variant<S, FB1, FB2, FB3, true>(a, maps, wp, err, nsm, st);
+    if (e != cudaSuccess) return e;
+    if (nlaunch) ++*nlaunch;
+  }
+  return cudaSuccess;
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
@@ -609,33 +731,18 @@ cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps_in, int 
   const int code = (a.fb1 > 0) * 4 + (a.fb2 > 0) * 2 + (a.fb3 > 0);
   cudaError_t e;
   switch (code) {
-    case 0: e = launch_one<S, -1, -1, -1>(a, m, err, counter, st); break;
-    case 1: e = launch_one<S, -1, -1, 1>(a, m, err, counter, st); break;
-    case 2: e = launch_one<S, -1, 1, -1>(a, m, err, counter, st); break;
-    case 3: e = launch_one<S, -1, 1, 1>(a, m, err, counter, st); break;
-    case 4: e = launch_one<S, 1, -1, -1>(a, m, err, counter, st); break;
-    case 5: e = launch_one<S, 1, -1, 1>(a, m, err, counter, st); break;
-    case 6: e = launch_one<S, 1, 1, -1>(a, m, err, counter, st); break;
-    default: e = launch_one<S, 1, 1, 1>(a, m, err, counter, st);
+    case 0: e = launch_one<S, -1, -1, -1>(a, m, err, counter, st, nlaunch); break;
+    case 1: e = launch_one<S, -1, -1, 1>(a, m, err, counter, st, nlaunch); break;
+    case 2: e = launch_one<S, -1, 1, -1>(a, m, err, counter, st, nlaunch); break;
+    case 3: e = launch_one<S, -1, 1, 1>(a, m, err, counter, st, nlaunch); break;
+    case 4: e = launch_one<S, 1, -1, -1>(a, m, err, counter, st, nlaunch); break;
+    case 5: e = launch_one<S, 1, -1, 1>(a, m, err, counter, st, nlaunch); break;
+    case 6: e = launch_one<S, 1, 1, -1>(a, m, err, counter, st, nlaunch); break;
+    default: e = launch_one<S, 1, 1, 1>(a, m, err, counter, st, nlaunch);
   }
   if (e != cudaSuccess) return e;
-  if (nlaunch) ++*nlaunch;
-  if (after_main) {
-    e = cudaEventRecord(after_main, st);
-    if (e != cudaSuccess) return e;
-  }
-  if (a.nslab == 0) return cudaSuccess;
-  for (int axis = 0; axis < 3; ++axis) {
-    const SlabDev<float> &s0 = a.slab[axis];
-    const int nk = std::min(s0.n2, a.kend - s0.off2);
-    if (nk <= 0) continue;
-    const long long n = (long long)s0.n0 * s0.n1 * nk * (axis == 2 ? 1 : 2);
-    pml_correct_kernel<S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, axis, a.kend);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    if (nlaunch) ++*nlaunch;
-  }
-  return cudaSuccess;
+  if (after_main) e = cudaEventRecord(after_main, st);
+  return e;
 }
 template <>
 cudaError_t launch_stage_stream<double>(const StageArgs<double> &, const void *, int *, int *,

@@ -157,9 +157,11 @@ int cgfdm_get_timing(cgfdm_handle *h, float *ms3);
 /* Per-kernel view of the last cgfdm_run (device events, timing enabled):
  * [0] streaming-kernel time in ms, [1] its launches, [2] the algorithmic
  * bytes those launches move (fields read and written once per point and
- * stage), [3] kernels launched by the run (counted whether or not timing is
- * on), [4] PML-correction time in ms, [5] exact-order (free-surface) kernel
- * time in ms, [6] stages timed, [7] reserved. */
+ * stage; the PML auxiliaries, handled inside the same kernel, are not
+ * counted), [3] kernels launched by the run (counted whether or not timing is
+ * on), [4] time between the streaming kernel and the exact-order kernel in
+ * ms (no kernel runs there), [5] exact-order (free-surface) kernel time in
+ * ms, [6] stages timed, [7] reserved. */
 int cgfdm_get_kernel_stats(cgfdm_handle *h, double *out8);
 
 /* ---- one RK stage without any device allocation ------------------------
