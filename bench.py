@@ -277,6 +277,8 @@ def main():
     ap.add_argument("--kernel", default="auto", choices=["auto", "exact", "stream"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--tile-rows", type=int, default=0, choices=[0, 8, 16],
+                    help="streaming-kernel tile height (0: the library's autotuner)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-steps", type=int, default=20)
     ap.add_argument("--accuracy-steps", type=int, default=0,
@@ -346,6 +348,7 @@ def main():
         desc = cgfdm.make_desc(desc0.nx, desc0.ny, desc0.nz, desc0.npml, desc0.dh, desc0.dt, nt,
                                prec, kern, local)
         sim = cgfdm.Simulation(desc)
+        sim.set_tile_rows(args.tile_rows)
         sim.set_model(cjm, setup["rdz"])
         if setup["point"] is not None:
             sim.set_point_source(*setup["point"], setup["rickerfc"])
@@ -457,7 +460,8 @@ def main():
             "data": "synthetic",
             "config": {"workload": w["name"], "precision": args.precision,
                        "grid": [desc0.nx, desc0.ny, desc0.nz], "points": npts,
-                       "kernel": args.kernel, "parallelism": "replicas" if ws > 1 else "single",
+                       "kernel": args.kernel, "tile_rows": ks["tile_rows"],
+                       "parallelism": "replicas" if ws > 1 else "single",
                        "l2": "inputs larger than L2 (%.2f GB per wavefield buffer), no flush" % (
                            9 * (desc0.nx + 6) * (desc0.ny + 6) * (desc0.nz + 6) *
                            {"fp32": 4, "fp64": 8}.get(args.precision, 2) / 1e9)},

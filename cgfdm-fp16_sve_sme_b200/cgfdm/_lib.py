@@ -80,6 +80,7 @@ SIGNATURES = {
     "cgfdm_set_timing": (C.c_int, [P, I32]),
     "cgfdm_get_timing": (C.c_int, [P, P]),
     "cgfdm_get_kernel_stats": (C.c_int, [P, P]),
+    "cgfdm_set_tile_rows": (C.c_int, [P, I32]),
     "cgfdm_propagate": (C.c_int, [C.POINTER(Desc), P, P, I32, P, F, P, P, I64, I32, F, P, I32,
                                   P, P, P]),
     "cgfdm_run_directory": (C.c_int, [C.c_char_p, I32, I32, I32]),

@@ -108,13 +108,17 @@ class Simulation:
         check(lib().cgfdm_get_timing(self._h, _ptr(ms)))
         return ms
 
+    def set_tile_rows(self, rows):
+        """Streaming-kernel tile height: 16, 8, or 0 to autotune at the first run."""
+        check(lib().cgfdm_set_tile_rows(self._h, int(rows)))
+
     def kernel_stats(self):
         """Per-kernel device view of the last run (cgfdm_get_kernel_stats)."""
         v = np.zeros(8, np.float64)
         check(lib().cgfdm_get_kernel_stats(self._h, _ptr(v)))
         return {"stream_ms": v[0], "stream_launches": int(v[1]), "stream_bytes": v[2],
                 "launches": int(v[3]), "gap_ms": v[4], "exact_ms": v[5],
-                "stages": int(v[6])}
+                "stages": int(v[6]), "tile_rows": int(v[7])}
 
     # ---- outputs ----------------------------------------------------------
     def stations(self):

@@ -182,6 +182,11 @@ int cgfdm_get_timing(cgfdm_handle *h, float *ms3) {
   return h->eng->get_timing(ms3);
 }
 
+int cgfdm_set_tile_rows(cgfdm_handle *h, int32_t rows) {
+  H_OR_FAIL(h);
+  return h->eng->set_tile_rows(rows);
+}
+
 int cgfdm_get_kernel_stats(cgfdm_handle *h, double *out8) {
   H_OR_FAIL(h);
   if (!out8) return CGFDM_ERR_ARG;

@@ -20,7 +20,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 
@@ -48,6 +51,11 @@ namespace {
 
 const int kFB[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1},  {-1, -1, 1},
                        {-1, 1, -1},  {1, -1, -1}, {1, -1, 1}, {-1, 1, 1}};
+
+// Autotuner results: streaming-kernel tile height per (precision, nx, ny, nz,
+// nPML), shared by every handle of the process.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int>, int> g_tuned;
 
 struct Dims {
   int nx, ny, nz, npml;
@@ -241,6 +249,10 @@ template <typename S> class EngineT : public Engine {
       return CGFDM_ERR_ARG;
     }
     last_stream_ = st;
+    if (use_stream_ && tile_rows_ == 0) {
+      int rc = tune(st);
+      if (rc) return rc;
+    }
     stage_used_ = 0;
     launches_ = 0;
     stream_bytes_ = 0.0;
@@ -412,6 +424,15 @@ template <typename S> class EngineT : public Engine {
 
   int set_timing(bool on) override { timing_ = on; return CGFDM_OK; }
 
+  int set_tile_rows(int rows) override {
+    if (rows != 0 && rows != 8 && rows != 16) {
+      set_error("tile rows must be 0 (autotune), 8 or 16");
+      return CGFDM_ERR_ARG;
+    }
+    tile_rows_ = rows;
+    return CGFDM_OK;
+  }
+
   int get_timing(float *ms3) override {
     // [0] the last run() end to end, [1] sum over its stage-kernel launches,
     // [2] the number of those launches
@@ -436,6 +457,7 @@ template <typename S> class EngineT : public Engine {
     if (rc) return rc;
     for (int q = 0; q < 8; ++q) out[q] = 0.0;
     out[3] = launches_;
+    out[7] = use_stream_ ? (tile_rows_ ? tile_rows_ : 16) : 0;
     if (!timing_) return CGFDM_OK;
     double part[3] = {0, 0, 0};
     for (int q = 0; q < stage_used_; ++q)
@@ -450,6 +472,7 @@ template <typename S> class EngineT : public Engine {
     out[4] = part[1];
     out[5] = part[2];
     out[6] = stage_used_;
+    out[7] = use_stream_ ? (tile_rows_ ? tile_rows_ : 16) : 0;
     return CGFDM_OK;
   }
 
@@ -466,9 +489,10 @@ template <typename S> class EngineT : public Engine {
     return e == cudaSuccess ? cudaStreamSynchronize(own_stream_) : e;
   }
 
-  int launch_stage(int irk, const int fb[3], cudaStream_t st) {
+  // Everything stage irk reads and writes (k range left to the caller).
+  StageArgs<S> stage_args(int irk, const int fb[3]) const {
     static const int in_of[4] = {0, 1, 2, 1}, out_of[4] = {1, 2, 1, 0};
-    S *bufs[3] = {A_, X_, Y_};
+    S *const bufs[3] = {A_, X_, Y_};
     StageArgs<S> a{};
     a.win = bufs[in_of[irk]];
     a.wout = bufs[out_of[irk]];
@@ -496,6 +520,62 @@ template <typename S> class EngineT : public Engine {
       sl.at = auxbuf(3) + off;
       off += g_.slab_pts[s] * 9;
     }
+    return a;
+  }
+
+  // Picks the streaming kernel's tile height for this grid and precision:
+  // times stage 0 at the current step boundary with each candidate (stage 0
+  // reads only the step state and writes buffers the next stage 0 rewrites)
+  // and keeps the fastest; results are cached per (precision, grid).
+  int tune(cudaStream_t st) {
+    const auto key = std::make_tuple((int)d_.precision, d_.nx, d_.ny, d_.nz, d_.npml);
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto f = g_tuned.find(key);
+      if (f != g_tuned.end()) {
+        tile_rows_ = f->second;
+        return CGFDM_OK;
+      }
+    }
+    const int fb[3] = {kFB[it_ % 8][0], kFB[it_ % 8][1], kFB[it_ % 8][2]};
+    StageArgs<S> b = stage_args(0, fb);
+    b.kbeg = HALO;
+    b.kend = g_.L.nz_ - HALO - 3;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    int best = 16;
+    float best_ms = 1e30f;
+    cudaError_t err = cudaSuccess;
+    for (int rows : {16, 8}) {
+      err = launch_stage_stream<S>(b, tmap_[0], err_flag_, err_flag_ + 1, st, nullptr, nullptr,
+                                   rows);
+      if (err == cudaSuccess) err = cudaEventRecord(e0, st);
+      for (int r = 0; r < 2 && err == cudaSuccess; ++r)
+        err = launch_stage_stream<S>(b, tmap_[0], err_flag_, err_flag_ + 1, st, nullptr,
+                                     nullptr, rows);
+      if (err == cudaSuccess) err = cudaEventRecord(e1, st);
+      if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+      float ms = 0;
+      if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+      if (err != cudaSuccess) break;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = rows;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CUDA_TRY(err);
+    tile_rows_ = best;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[key] = best;
+    return CGFDM_OK;
+  }
+
+  int launch_stage(int irk, const int fb[3], cudaStream_t st) {
+    static const int in_of[4] = {0, 1, 2, 1}, out_of[4] = {1, 2, 1, 0};
+    StageArgs<S> a = stage_args(irk, fb);
     last_out_ = a.wout;
     last_aux_out_ = aux_total_ > 0 ? auxbuf(out_of[irk]) : nullptr;
     // events per timed stage: [0] start, [1] after the streaming kernel,
@@ -516,7 +596,8 @@ template <typename S> class EngineT : public Engine {
       b.kbeg = HALO;
       b.kend = ksurf;
       CUDA_TRY(launch_stage_stream<S>(b, tmap_[in_of[irk]], err_flag_, err_flag_ + 1, st,
-                                      ev ? ev[1] : nullptr, &launches_));
+                                      ev ? ev[1] : nullptr, &launches_,
+                                      tile_rows_ ? tile_rows_ : 16));
       if (ev) CUDA_TRY(cudaEventRecord(ev[2], st));
       // fields read and written per point by this stage: W in, 12 coefficients,
       // W out, plus m (stages 1, 2) and t (written in 0, updated in 1-2, read in 3)
@@ -618,6 +699,7 @@ template <typename S> class EngineT : public Engine {
   std::vector<cudaEvent_t> stage_ev_;
   int stage_used_ = 0;
   int launches_ = 0;          // kernels launched by the last run()
+  int tile_rows_ = 0;         // streaming-kernel tile height; 0 = autotune at the first run()
   double stream_bytes_ = 0;   // algorithmic bytes of its streaming-kernel launches
 };
 

@@ -37,6 +37,7 @@ class Engine {
   virtual int set_timing(bool on) = 0;
   virtual int get_timing(float *ms3) = 0;
   virtual int get_kernel_stats(double *out8) = 0;
+  virtual int set_tile_rows(int rows) = 0;
   virtual const cgfdm_desc &desc() const = 0;
 };
 

@@ -22,14 +22,16 @@ template <typename S> cudaError_t launch_stage_exact(const StageArgs<S> &a, cuda
 // TMA-staged z-streaming fused stage over kbeg <= k < kend, which must lie
 // below the three free-surface layers.  `maps` holds the tensor maps of the
 // stage input wavefield and of the coefficients (encode_stream_maps).
-constexpr int kStreamMapsBytes = 640;
+constexpr int kStreamMapsBytes = 1280;
 // `after_main` (optional) is recorded right after the streaming kernel,
 // before the exact-order kernel; `nlaunch` (optional) is increased by the
-// number of kernels launched.
+// number of kernels launched; `tile_rows` (16 or 8) selects the tile height
+// (32 x 16 tiles, one CTA per SM; or 32 x 8, two CTAs per SM).
 template <typename S>
 cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps, int *err_flag,
                                 int *work_counter, cudaStream_t st,
-                                cudaEvent_t after_main = nullptr, int *nlaunch = nullptr);
+                                cudaEvent_t after_main = nullptr, int *nlaunch = nullptr,
+                                int tile_rows = 16);
 template <typename S> bool stage_stream_supported();
 // Encodes the tensor maps the streaming kernel loads its tiles through (the
 // 9 wavefield components of the stage input `wave`, the 13 coefficient

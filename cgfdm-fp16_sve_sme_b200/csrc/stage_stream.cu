@@ -45,11 +45,16 @@
 namespace cgfdm {
 namespace {
 
-constexpr int TX = 32, TY = 16, NTHR = TX * TY;
-constexpr int BY = TY + 4;  // y box: 1 or 3 rows before the tile, 3 or 1 after
+constexpr int TX = 32;
 constexpr long long kWaitCycles = 1LL << 31;
 
-template <typename S> struct Geo {
+// Tile and shared-memory geometry for storage type S and tile height TYv
+// (16: one 512-thread CTA per SM; 8: 256-thread CTAs, two per SM when their
+// shared memory fits, so one CTA's per-plane barrier overlaps the other's work).
+template <typename S, int TYv> struct Geo {
+  static constexpr int TY = TYv, NTHR = TX * TYv;
+  static constexpr int BY = TYv + 4;  // y box: 1 or 3 rows before the tile, 3 or 1 after
+  static constexpr int MINB = TYv == 8 ? 2 : 1;
   static constexpr int ES = (int)sizeof(S);
   static constexpr int HB = 16 / ES;                             // elements per 16 bytes
   static constexpr int BX = ((HB + TX + 3) + HB - 1) / HB * HB;  // x box, aligned origin
@@ -237,10 +242,13 @@ __device__ __forceinline__ void pml_warp(unsigned vm, const SlabDev<float> &sl, 
 
 struct Maps {
   CUtensorMap w;   // stage input wavefield, box BX x BY x 1 x 9
-  CUtensorMap c9;  // coefficients, box 32 x 16 x 1 x 9 (metrics)
-  CUtensorMap c3;  // coefficients, box 32 x 16 x 1 x 3 (mu, lambda, b at field 10)
-  CUtensorMap m;   // step-start wavefield, box 32 x 16 x 1 x 9
-  CUtensorMap t;   // RK accumulator, box 32 x 16 x 1 x 9
+  CUtensorMap c9;  // coefficients, box 32 x TY x 1 x 9 (metrics)
+  CUtensorMap c3;  // coefficients, box 32 x TY x 1 x 3 (mu, lambda, b at field 10)
+  CUtensorMap m;   // step-start wavefield, box 32 x TY x 1 x 9
+  CUtensorMap t;   // RK accumulator, box 32 x TY x 1 x 9
+};
+struct MapSet {
+  Maps ty16, ty8;  // the same buffers, boxes for tile heights 16 and 8
 };
 
 // Work items of one launch.  The z range [kbeg, kend) is cut at kz, the top
@@ -306,11 +314,12 @@ __device__ __forceinline__ void item_of(const Work &w, int item, int &bxi, int &
   }
 }
 
-template <typename S, int FB1, int FB2, int FB3, bool PMLK>
-__global__ void __launch_bounds__(NTHR, 1)
+template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK>
+__global__ void __launch_bounds__(TX * TYv, Geo<S, TYv>::MINB)
     stage_stream_kernel(const __grid_constant__ Maps maps, const StageArgs<S> a, const Work wk,
                         int *err) {
-  using G = Geo<S>;
+  using G = Geo<S, TYv>;
+  constexpr int TY = G::TY, NTHR = G::NTHR, BY = G::BY;
   constexpr int NW = G::NW, NC = G::NC, NM = G::NM, BX = G::BX;
   constexpr int DIR = -FB3;  // sweep direction in z
   extern __shared__ unsigned char smem_raw[];
@@ -576,12 +585,13 @@ __global__ void __launch_bounds__(NTHR, 1)
   }
 }
 
-template <typename S, int FB1, int FB2, int FB3, bool PMLK>
+template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK>
 cudaError_t launch_variant(const StageArgs<S> &a, const Maps &maps, const Work &wk, int *err,
                            int nsm, cudaStream_t st) {
+  using G = Geo<S, TYv>;
   static int attr_dev = -1;
-  auto kern = stage_stream_kernel<S, FB1, FB2, FB3, PMLK>;
-  const int smem = PMLK ? Geo<S>::SMEM_P : Geo<S>::SMEM;
+  auto kern = stage_stream_kernel<S, TYv, FB1, FB2, FB3, PMLK>;
+  const int smem = PMLK ? G::SMEM_P : G::SMEM;
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
@@ -592,15 +602,17 @@ cudaError_t launch_variant(const StageArgs<S> &a, const Maps &maps, const Work &
   }
   cudaError_t e = cudaMemsetAsync(wk.counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
-  kern<<<std::min(wk.nitems, nsm), NTHR, smem, st>>>(maps, a, wk, err);
+  kern<<<std::min(wk.nitems, nsm * G::MINB), G::NTHR, smem, st>>>(maps, a, wk, err);
   return cudaGetLastError();
 }
 
 // Splits the stage into the interior launch (tiles and chunks that touch no
 // PML slab) and the PML launch (the rest), see Work.
-template <typename S, int FB1, int FB2, int FB3>
+template <typename S, int TYv, int FB1, int FB2, int FB3>
 cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *counter,
                        cudaStream_t st, int *nlaunch) {
+  constexpr int TY = TYv;
+  constexpr int slots = Geo<S, TYv>::MINB;  // CTAs resident per SM
   static int nsm = 0;
   if (!nsm) {
     int dev = 0;
@@ -631,7 +643,7 @@ cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *c
   wk.nzc = pl_p > 0 ? (pl_p + 31) / 32 : 0;
   wk.chunk_p = wk.nzc ? (pl_p + wk.nzc - 1) / wk.nzc : 1;
   // upper planes: about 24 items per SM, chunks of at least 24 planes
-  int nic = pl_i > 0 ? (24 * nsm + tiles - 1) / tiles : 0;
+  int nic = pl_i > 0 ? (24 * nsm * slots + tiles - 1) / tiles : 0;
   if (pl_i > 0) nic = std::max(1, std::min(nic, pl_i / 24));
   wk.chunk_i = nic ? (pl_i + nic - 1) / nic : 1;
   wk.nic = nic ? (pl_i + wk.chunk_i - 1) / wk.chunk_i : 0;
@@ -639,14 +651,14 @@ cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *c
   Work wi = wk;
   wi.nitems = tiles_in * wk.nic;
   if (wi.nitems > 0) {
-    e = launch_variant<S, FB1, FB2, FB3, false>(a, maps, wi, err, nsm, st);
+    e = launch_variant<S, TYv, FB1, FB2, FB3, false>(a, maps, wi, err, nsm, st);
     if (e != cudaSuccess) return e;
     if (nlaunch) ++*nlaunch;
   }
   Work wp = wk;
   wp.nitems = wk.nzc * tiles + (tiles - tiles_in) * wk.nic;
   if (wp.nitems > 0) {
-    e = launch_variant<S, FB1, FB2, FB3, true>(a, maps, wp, err, nsm, st);
+    e = launch_variant<S, TYv, FB1, FB2, FB3, true>(a, maps, wp, err, nsm, st);
     if (e != cudaSuccess) return e;
     if (nlaunch) ++*nlaunch;
   }
@@ -706,14 +718,18 @@ template <> bool stage_stream_supported<double>() { return false; }
 template <typename S>
 int encode_stream_maps(const S *wave, const S *cjm, const S *wm, const S *t, const Layout &L,
                        void *out) {
-  static_assert(sizeof(Maps) <= kStreamMapsBytes, "tensor-map buffer too small");
-  Maps m;
-  int rc = encode_map<S>(wave, L, 9, Geo<S>::BX, BY, 9, &m.w);
-  if (!rc) rc = encode_map<S>(cjm, L, 13, TX, TY, 9, &m.c9);
-  if (!rc) rc = encode_map<S>(cjm, L, 13, TX, TY, 3, &m.c3);
-  if (!rc) rc = encode_map<S>(wm, L, 9, TX, TY, 9, &m.m);
-  if (!rc) rc = encode_map<S>(t, L, 9, TX, TY, 9, &m.t);
-  if (!rc) std::memcpy(out, &m, sizeof m);
+  static_assert(sizeof(MapSet) <= kStreamMapsBytes, "tensor-map buffer too small");
+  MapSet ms;
+  int rc = CGFDM_OK;
+  for (int ty : {16, 8}) {
+    Maps &m = ty == 16 ? ms.ty16 : ms.ty8;
+    if (!rc) rc = encode_map<S>(wave, L, 9, Geo<S, 16>::BX, ty + 4, 9, &m.w);
+    if (!rc) rc = encode_map<S>(cjm, L, 13, TX, ty, 9, &m.c9);
+    if (!rc) rc = encode_map<S>(cjm, L, 13, TX, ty, 3, &m.c3);
+    if (!rc) rc = encode_map<S>(wm, L, 9, TX, ty, 9, &m.m);
+    if (!rc) rc = encode_map<S>(t, L, 9, TX, ty, 9, &m.t);
+  }
+  if (!rc) std::memcpy(out, &ms, sizeof ms);
   return rc;
 }
 template <>
@@ -723,30 +739,37 @@ int encode_stream_maps<double>(const double *, const double *, const double *, c
   return CGFDM_ERR_ARG;
 }
 
+template <typename S, int TYv>
+cudaError_t launch_fb(const StageArgs<S> &a, const Maps &m, int *err, int *counter,
+                      cudaStream_t st, int *nlaunch) {
+  const int code = (a.fb1 > 0) * 4 + (a.fb2 > 0) * 2 + (a.fb3 > 0);
+  switch (code) {
+    case 0: return launch_one<S, TYv, -1, -1, -1>(a, m, err, counter, st, nlaunch);
+    case 1: return launch_one<S, TYv, -1, -1, 1>(a, m, err, counter, st, nlaunch);
+    case 2: return launch_one<S, TYv, -1, 1, -1>(a, m, err, counter, st, nlaunch);
+    case 3: return launch_one<S, TYv, -1, 1, 1>(a, m, err, counter, st, nlaunch);
+    case 4: return launch_one<S, TYv, 1, -1, -1>(a, m, err, counter, st, nlaunch);
+    case 5: return launch_one<S, TYv, 1, -1, 1>(a, m, err, counter, st, nlaunch);
+    case 6: return launch_one<S, TYv, 1, 1, -1>(a, m, err, counter, st, nlaunch);
+    default: return launch_one<S, TYv, 1, 1, 1>(a, m, err, counter, st, nlaunch);
+  }
+}
+
 template <typename S>
 cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps_in, int *err, int *counter,
-                                cudaStream_t st, cudaEvent_t after_main, int *nlaunch) {
+                                cudaStream_t st, cudaEvent_t after_main, int *nlaunch,
+                                int tile_rows) {
   if (a.kend <= a.kbeg) return cudaSuccess;
-  const Maps &m = *(const Maps *)maps_in;
-  const int code = (a.fb1 > 0) * 4 + (a.fb2 > 0) * 2 + (a.fb3 > 0);
-  cudaError_t e;
-  switch (code) {
-    case 0: e = launch_one<S, -1, -1, -1>(a, m, err, counter, st, nlaunch); break;
-    case 1: e = launch_one<S, -1, -1, 1>(a, m, err, counter, st, nlaunch); break;
-    case 2: e = launch_one<S, -1, 1, -1>(a, m, err, counter, st, nlaunch); break;
-    case 3: e = launch_one<S, -1, 1, 1>(a, m, err, counter, st, nlaunch); break;
-    case 4: e = launch_one<S, 1, -1, -1>(a, m, err, counter, st, nlaunch); break;
-    case 5: e = launch_one<S, 1, -1, 1>(a, m, err, counter, st, nlaunch); break;
-    case 6: e = launch_one<S, 1, 1, -1>(a, m, err, counter, st, nlaunch); break;
-    default: e = launch_one<S, 1, 1, 1>(a, m, err, counter, st, nlaunch);
-  }
+  const MapSet &ms = *(const MapSet *)maps_in;
+  cudaError_t e = tile_rows == 8 ? launch_fb<S, 8>(a, ms.ty8, err, counter, st, nlaunch)
+                                 : launch_fb<S, 16>(a, ms.ty16, err, counter, st, nlaunch);
   if (e != cudaSuccess) return e;
   if (after_main) e = cudaEventRecord(after_main, st);
   return e;
 }
 template <>
 cudaError_t launch_stage_stream<double>(const StageArgs<double> &, const void *, int *, int *,
-                                        cudaStream_t, cudaEvent_t, int *) {
+                                        cudaStream_t, cudaEvent_t, int *, int) {
   return cudaErrorNotSupported;
 }
 
@@ -761,10 +784,10 @@ template int encode_stream_maps<__nv_bfloat16>(const __nv_bfloat16 *, const __nv
                                                const __nv_bfloat16 *, const __nv_bfloat16 *,
                                                const Layout &, void *);
 template cudaError_t launch_stage_stream<float>(const StageArgs<float> &, const void *, int *,
-                                                int *, cudaStream_t, cudaEvent_t, int *);
+                                                int *, cudaStream_t, cudaEvent_t, int *, int);
 template cudaError_t launch_stage_stream<__half>(const StageArgs<__half> &, const void *, int *,
-                                                 int *, cudaStream_t, cudaEvent_t, int *);
+                                                 int *, cudaStream_t, cudaEvent_t, int *, int);
 template cudaError_t launch_stage_stream<__nv_bfloat16>(const StageArgs<__nv_bfloat16> &,
-                                                        const void *, int *, int *, cudaStream_t, cudaEvent_t, int *);
+                                                        const void *, int *, int *, cudaStream_t, cudaEvent_t, int *, int);
 
 }  // namespace cgfdm

@@ -161,8 +161,15 @@ int cgfdm_get_timing(cgfdm_handle *h, float *ms3);
  * counted), [3] kernels launched by the run (counted whether or not timing is
  * on), [4] time between the streaming kernel and the exact-order kernel in
  * ms (no kernel runs there), [5] exact-order (free-surface) kernel time in
- * ms, [6] stages timed, [7] reserved. */
+ * ms, [6] stages timed, [7] the streaming kernel's tile height (0: not used). */
 int cgfdm_get_kernel_stats(cgfdm_handle *h, double *out8);
+
+/* Tile height of the streaming kernel: 16 (32 x 16 tiles, one CTA per SM),
+ * 8 (32 x 8 tiles, two CTAs per SM), or 0 (the default): autotune -- the
+ * first cgfdm_run times one stage with each height on this handle's buffers
+ * (blocking that call for a few stage times) and keeps the fastest; the
+ * choice is cached per (precision, grid) for the process. */
+int cgfdm_set_tile_rows(cgfdm_handle *h, int32_t rows);
 
 /* ---- one RK stage without any device allocation ------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc

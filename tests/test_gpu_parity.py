@@ -67,11 +67,12 @@ def test_stage_bitwise(stage_golden, case):
         off += 3 * n9
 
 
-def _run_sim(g, precision=None, kernel=None, steps=None):
+def _run_sim(g, precision=None, kernel=None, steps=None, tile_rows=0):
     p = g["params"]
     nt = scenarios.S.nt_of(p)
     steps = nt if steps is None else steps
     sim = cgfdm.Simulation(_desc(p, nt, precision, kernel))
+    sim.set_tile_rows(tile_rows)
     sim.set_model(g["cjm"], g["rdz"])
     if p["useMultiSource"]:
         dt = float(np.frombuffer(g["source"][8:12].tobytes(), np.float32)[0])

@@ -7,6 +7,7 @@ rounding rather than bit for bit.  Tolerances (relative L2 norms):
     reference's increment, per field, and the PML auxiliaries within 1e-5;
   * complete runs: station seismograms within 1e-5 of the reference's and
     the PGV map within 1e-5.
+Both tile heights of the kernel (32 x 16 and 32 x 8) are checked.
 """
 import numpy as np
 import pytest
@@ -29,12 +30,14 @@ def stage_golden(gpu_available):
     return scenarios.load_golden("stage_small.npz")
 
 
+@pytest.mark.parametrize("rows", [16, 8])
 @pytest.mark.parametrize("case", range(len(scenarios.STAGE_CASES)))
-def test_stream_stage_matches_reference(stage_golden, case):
+def test_stream_stage_matches_reference(stage_golden, case, rows):
     g = stage_golden
     p = g["params"]
     irk, fb = scenarios.STAGE_CASES[case]
     with cgfdm.Simulation(_desc(p, 1, kernel=cgfdm.KERNEL_STREAM)) as sim:
+        sim.set_tile_rows(rows)
         sim.set_model(g["cjm"], g["rdz"])
         sim.set_state(irk, W=g["in_W"], t=g["in_t"], m=g["in_m"], aux=g["in_aux"])
         sim.stage(irk, fb)
@@ -53,10 +56,11 @@ def test_stream_stage_matches_reference(stage_golden, case):
         off += 3 * n9
 
 
+@pytest.mark.parametrize("rows", [16, 8])
 @pytest.mark.parametrize("name", ["run_point.npz", "run_fault.npz"])
-def test_stream_full_run_matches_reference(gpu_available, name):
+def test_stream_full_run_matches_reference(gpu_available, name, rows):
     g = scenarios.load_golden(name)
-    res = _run_sim(g, kernel=cgfdm.KERNEL_STREAM)
+    res = _run_sim(g, kernel=cgfdm.KERNEL_STREAM, tile_rows=rows)
     for v in range(9):
         err = rel_l2(res["station_wave"][:, :, v], g["out_station_wave"][:, :, v])
         assert err < 1e-5, (v, err)
@@ -64,7 +68,8 @@ def test_stream_full_run_matches_reference(gpu_available, name):
     assert rel_l2(res["freesurf"], g["out_freesurf"]) < 1e-5
 
 
-def test_stream_matches_exact_on_larger_grid(gpu_available):
+@pytest.mark.parametrize("rows", [16, 8, 0])
+def test_stream_matches_exact_on_larger_grid(gpu_available, rows):
     """A grid with several tiles in x and y, odd sizes (partial warps and
     tiles), several z chunks and all PML slabs: the fast path against the
     exact path (which is bit-identical to the reference), after 20 steps."""
@@ -85,6 +90,7 @@ def test_stream_matches_exact_on_larger_grid(gpu_available):
     out = {}
     for kern in (cgfdm.KERNEL_EXACT, cgfdm.KERNEL_STREAM):
         with cgfdm.Simulation(_desc(p, 20, kernel=kern)) as sim:
+            sim.set_tile_rows(rows)
             sim.set_model(cjm.reshape(-1), rdz)
             sim.set_point_source(nx // 2, ny // 2, nz // 2, 6.0)
             sim.set_stations(sta)
