@@ -81,6 +81,12 @@ SIGNATURES = {
     "cgfdm_get_timing": (C.c_int, [P, P]),
     "cgfdm_get_kernel_stats": (C.c_int, [P, P]),
     "cgfdm_set_tile_rows": (C.c_int, [P, I32]),
+    "cgfdm_set_graph": (C.c_int, [P, I32]),
+    "cgfdm_batch_create": (C.c_int, [P, I32, C.POINTER(P)]),
+    "cgfdm_batch_run": (C.c_int, [P, I32, P]),
+    "cgfdm_batch_set_graph": (C.c_int, [P, I32]),
+    "cgfdm_batch_synchronize": (C.c_int, [P]),
+    "cgfdm_batch_destroy": (C.c_int, [P]),
     "cgfdm_propagate": (C.c_int, [C.POINTER(Desc), P, P, I32, P, F, P, P, I64, I32, F, P, I32,
                                   P, P, P]),
     "cgfdm_run_directory": (C.c_int, [C.c_char_p, I32, I32, I32]),

@@ -108,6 +108,10 @@ class Simulation:
         check(lib().cgfdm_get_timing(self._h, _ptr(ms)))
         return ms
 
+    def set_graph(self, on=True):
+        """Replay each step of run() as a CUDA graph (results are identical)."""
+        check(lib().cgfdm_set_graph(self._h, int(on)))
+
     def set_tile_rows(self, rows):
         """Streaming-kernel tile height: 16, 8, or 0 to autotune at the first run."""
         check(lib().cgfdm_set_tile_rows(self._h, int(rows)))
@@ -158,6 +162,45 @@ class Simulation:
         aux = np.zeros(3 * self.aux_floats(), np.float32)
         check(lib().cgfdm_get_state(self._h, _ptr(W), _ptr(t), _ptr(m), _ptr(aux)))
         return {"W": W, "t": t, "m": m, "aux": aux}
+
+
+class Batch:
+    """Several Simulations of one precision advanced together (cgfdm_batch):
+    one persistent streaming launch per stage spans all members.  The
+    members must outlive the batch; read results from the members after
+    synchronize()."""
+
+    def __init__(self, sims, graph=False):
+        self.sims = list(sims)
+        arr = (C.c_void_p * len(self.sims))(*[s._h.value for s in self.sims])
+        b = C.c_void_p()
+        check(lib().cgfdm_batch_create(arr, len(self.sims), C.byref(b)))
+        self._b = b
+        if graph:
+            check(lib().cgfdm_batch_set_graph(self._b, 1))
+
+    def run(self, nsteps, stream=None):
+        check(lib().cgfdm_batch_run(self._b, int(nsteps), stream))
+
+    def synchronize(self):
+        check(lib().cgfdm_batch_synchronize(self._b))
+
+    def close(self):
+        if getattr(self, "_b", None):
+            lib().cgfdm_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def propagate(desc, cjm, rdz, *, point=None, rickerfc=0.0, src_index=None, moment_rate=None,
@@ -254,5 +297,5 @@ def run_directory(run_dir, precision=_lib.FP32, kernel=_lib.KERNEL_AUTO, device=
     check(lib().cgfdm_run_directory(run_dir.encode(), precision, kernel, device))
 
 
-__all__ = ["Simulation", "propagate", "setup_from_directory", "run_directory", "make_desc",
+__all__ = ["Simulation", "Batch", "propagate", "setup_from_directory", "run_directory", "make_desc",
            "device_bytes", "CgfdmError", "hbm_layout", "stage_noalloc"]

@@ -8,10 +8,12 @@ namespace {
 
 template <typename S>
 __global__ void point_source_kernel(S *w0, S *w1, S *w2, const S *cjm, Layout L, int sx, int sy,
-                                    int sz, const float *amp343, float s, float DH3, double CsDT) {
+                                    int sz, const float *amp343, const float *moment,
+                                    const int *step, float DH3, double CsDT) {
   using R = typename Arith<S>::R;
   const int t = threadIdx.x;
   if (t >= 343) return;
+  const float s = moment[*step];
   const int i = sx - 3 + t % 7, j = sy - 3 + (t / 7) % 7, k = sz - 3 + t / 49;
   const long long c = L.at(i, j, k);
   const float jacb = ldv(cjm + L.at(sx, sy, sz) + L.fs * 9);
@@ -32,9 +34,12 @@ __global__ void point_source_kernel(S *w0, S *w1, S *w2, const S *cjm, Layout L,
 
 template <typename S>
 __global__ void fault_source_kernel(S *w, long long fs, const long long *idx, const float *rate,
-                                    long long npts, int srcIt, float tw, float DT) {
+                                    long long npts, const int *src_it, const float *src_tw,
+                                    const int *step, float DT) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= npts) return;
+  const int srcIt = src_it[*step];
+  if (p >= npts || srcIt < 0) return;  // srcIt < 0: the source has ended
+  const float tw = src_tw[*step];
   const float *m0 = rate + ((long long)srcIt * npts + p) * 6;
   const float *m1 = rate + ((long long)(srcIt + 1) * npts + p) * 6;
   const long long c = idx[p];
@@ -46,9 +51,11 @@ __global__ void fault_source_kernel(S *w, long long fs, const long long *idx, co
 }
 
 template <typename S>
-__global__ void station_pgv_kernel(const S *w, Layout L, const int *xyz, int nsta, int NT, int it,
-                                   float *wave, float *pgv, float c1, float c2, double cv_inv) {
+__global__ void station_pgv_kernel(const S *w, Layout L, const int *xyz, int nsta, int NT,
+                                   const int *step, float *wave, float *pgv, float c1, float c2,
+                                   double cv_inv) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int it = *step;
   const int nx = L.nx_ - 2 * HALO, ny = L.ny_ - 2 * HALO;
   if (t < nsta) {
     const long long c = L.at(xyz[3 * t], xyz[3 * t + 1], xyz[3 * t + 2]);
@@ -67,6 +74,8 @@ __global__ void station_pgv_kernel(const S *w, Layout L, const int *xyz, int nst
     if (pgv[2 * t + 1] < vv) pgv[2 * t + 1] = vv;
   }
 }
+
+__global__ void step_advance_kernel(int *step) { *step += 1; }
 
 template <typename S>
 __global__ void slice_pack_kernel(const S *f, Layout L, int axis, int at, double c, float *out) {
@@ -114,29 +123,36 @@ __global__ void repack_out_kernel(const S *src, float *dst, Layout L, int nfield
 
 template <typename S>
 cudaError_t launch_point_source(S *w0, S *w1, S *w2, const S *cjm, Layout L, int sx, int sy,
-                                int sz, const float *amp343, float s, float DH3, double CsDT,
-                                cudaStream_t st) {
-  point_source_kernel<S><<<1, 352, 0, st>>>(w0, w1, w2, cjm, L, sx, sy, sz, amp343, s, DH3, CsDT);
+                                int sz, const float *amp343, const float *moment, const int *step,
+                                float DH3, double CsDT, cudaStream_t st) {
+  point_source_kernel<S><<<1, 352, 0, st>>>(w0, w1, w2, cjm, L, sx, sy, sz, amp343, moment, step,
+                                            DH3, CsDT);
   return cudaGetLastError();
 }
 
 template <typename S>
 cudaError_t launch_fault_source(S *w, long long fs, const long long *idx, const float *rate,
-                                long long npts, int srcIt, float tw, float DT, cudaStream_t st) {
+                                long long npts, const int *src_it, const float *src_tw,
+                                const int *step, float DT, cudaStream_t st) {
   if (npts <= 0) return cudaSuccess;
   fault_source_kernel<S><<<(unsigned)((npts + 255) / 256), 256, 0, st>>>(w, fs, idx, rate, npts,
-                                                                        srcIt, tw, DT);
+                                                                        src_it, src_tw, step, DT);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step_advance(int *step, cudaStream_t st) {
+  step_advance_kernel<<<1, 1, 0, st>>>(step);
   return cudaGetLastError();
 }
 
 template <typename S>
-cudaError_t launch_station_pgv(const S *w, Layout L, const int *xyz, int nsta, int NT, int it,
-                               float *wave, float *pgv, float c1, float c2, double cv_inv,
-                               cudaStream_t st) {
+cudaError_t launch_station_pgv(const S *w, Layout L, const int *xyz, int nsta, int NT,
+                               const int *step, float *wave, float *pgv, float c1, float c2,
+                               double cv_inv, cudaStream_t st) {
   const int n = (L.nx_ - 2 * HALO) * (L.ny_ - 2 * HALO);
   const int total = n > nsta ? n : nsta;
-  station_pgv_kernel<S><<<(total + 255) / 256, 256, 0, st>>>(w, L, xyz, nsta, NT, it, wave, pgv, c1,
-                                                             c2, cv_inv);
+  station_pgv_kernel<S><<<(total + 255) / 256, 256, 0, st>>>(w, L, xyz, nsta, NT, step, wave, pgv,
+                                                             c1, c2, cv_inv);
   return cudaGetLastError();
 }
 
@@ -162,11 +178,13 @@ cudaError_t launch_repack_out(const S *src, float *dst, Layout L, int nfield, cu
 
 #define CGFDM_INST(S)                                                                              \
   template cudaError_t launch_point_source<S>(S *, S *, S *, const S *, Layout, int, int, int,     \
-                                              const float *, float, float, double, cudaStream_t);  \
+                                              const float *, const float *, const int *, float,    \
+                                              double, cudaStream_t);                               \
   template cudaError_t launch_fault_source<S>(S *, long long, const long long *, const float *,    \
-                                              long long, int, float, float, cudaStream_t);         \
-  template cudaError_t launch_station_pgv<S>(const S *, Layout, const int *, int, int, int,        \
-                                             float *, float *, float, float, double,               \
+                                              long long, const int *, const float *, const int *,  \
+                                              float, cudaStream_t);                                \
+  template cudaError_t launch_station_pgv<S>(const S *, Layout, const int *, int, int,             \
+                                             const int *, float *, float *, float, float, double,  \
                                              cudaStream_t);                                        \
   template cudaError_t launch_slice_pack<S>(const S *, Layout, int, int, double, float *,         \
                                             cudaStream_t);                                         \

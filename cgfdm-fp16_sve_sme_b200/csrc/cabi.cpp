@@ -16,6 +16,10 @@ struct cgfdm_handle {
   std::unique_ptr<cgfdm::Engine> eng;
 };
 
+struct cgfdm_batch {
+  std::unique_ptr<cgfdm::BatchBase> b;
+};
+
 using cgfdm::set_error;
 
 namespace {
@@ -180,6 +184,52 @@ int cgfdm_get_timing(cgfdm_handle *h, float *ms3) {
   H_OR_FAIL(h);
   if (!ms3) return CGFDM_ERR_ARG;
   return h->eng->get_timing(ms3);
+}
+
+int cgfdm_set_graph(cgfdm_handle *h, int32_t on) {
+  H_OR_FAIL(h);
+  return h->eng->set_graph(on != 0);
+}
+
+int cgfdm_batch_create(cgfdm_handle *const *hs, int32_t n, cgfdm_batch **out) {
+  if (!hs || n <= 0 || !out) return CGFDM_ERR_ARG;
+  *out = nullptr;
+  return guarded([&] {
+    std::vector<cgfdm::Engine *> e;
+    for (int q = 0; q < n; ++q) {
+      int rc = check(hs[q]);
+      if (rc) return rc;
+      e.push_back(hs[q]->eng.get());
+    }
+    auto *b = new cgfdm_batch();
+    int rc = cgfdm::make_batch(e.data(), n, b->b);
+    if (rc) {
+      delete b;
+      return rc;
+    }
+    *out = b;
+    return CGFDM_OK;
+  });
+}
+
+int cgfdm_batch_run(cgfdm_batch *b, int32_t nsteps, void *stream) {
+  if (!b || !b->b || nsteps < 0) return CGFDM_ERR_ARG;
+  return b->b->run(nsteps, stream);
+}
+
+int cgfdm_batch_set_graph(cgfdm_batch *b, int32_t on) {
+  if (!b || !b->b) return CGFDM_ERR_ARG;
+  return b->b->set_graph(on != 0);
+}
+
+int cgfdm_batch_synchronize(cgfdm_batch *b) {
+  if (!b || !b->b) return CGFDM_ERR_ARG;
+  return b->b->synchronize();
+}
+
+int cgfdm_batch_destroy(cgfdm_batch *b) {
+  delete b;
+  return CGFDM_OK;
 }
 
 int cgfdm_set_tile_rows(cgfdm_handle *h, int32_t rows) {

@@ -87,8 +87,11 @@ Dims make_dims(const cgfdm_desc &d) {
   return m;
 }
 
+template <typename S> class BatchT;
+
 template <typename S> class EngineT : public Engine {
   using R = typename Arith<S>::R;
+  friend class BatchT<S>;
 
  public:
   explicit EngineT(const cgfdm_desc &d) : d_(d), g_(make_dims(d)) {}
@@ -125,6 +128,9 @@ template <typename S> class EngineT : public Engine {
     // [0] device error flag of the streaming kernel, [1] its work-queue counter
     CUDA_TRY(cudaMalloc(&err_flag_, 2 * sizeof(int)));
     CUDA_TRY(cudaMemsetAsync(err_flag_, 0, 2 * sizeof(int), own_stream_));
+    // the device copy of the step counter it_ (read by the per-step kernels)
+    CUDA_TRY(cudaMalloc(&step_, sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(step_, 0, sizeof(int), own_stream_));
     for (int q = 0; q < 2; ++q) CUDA_TRY(cudaEventCreate(&ev_[q]));
     use_stream_ = stage_stream_supported<S>() && d_.kernel != CGFDM_KERNEL_EXACT &&
                   g_.nz > 3;
@@ -159,6 +165,7 @@ template <typename S> class EngineT : public Engine {
     if (sx < HALO || sx >= L.nx_ - HALO || sy < HALO || sy >= L.ny_ - HALO || sz < HALO ||
         sz >= L.nz_ - HALO) {
       point_on_ = false;  // singleSource.cpp:157-164: a source outside the rank is skipped
+      drop_graphs();
       return CGFDM_OK;
     }
     if (sx - 3 < 0 || sy - 3 < 0 || sz - 3 < 0 || sx + 3 >= L.nx_ || sy + 3 >= L.ny_ ||
@@ -166,9 +173,18 @@ template <typename S> class EngineT : public Engine {
       set_error("point source 7^3 smoothing window leaves the padded grid");
       return CGFDM_ERR_SOURCE;
     }
+    CUDA_TRY(cudaSetDevice(d_.device));
+    // moment of every step (singleSource.cpp:29-56), evaluated on the host
+    std::vector<float> tab(d_.nt > 0 ? d_.nt : 1);
+    for (int it = 0; it < d_.nt; ++it) tab[it] = ricker_moment(rickerfc, it, d_.dt);
+    if (moment_tab_) cudaFree(moment_tab_);
+    moment_tab_ = nullptr;
+    CUDA_TRY(cudaMalloc(&moment_tab_, sizeof(float) * tab.size()));
+    CUDA_TRY(h2d(moment_tab_, tab.data(), sizeof(float) * tab.size()));
     point_on_ = true;
     psrc_[0] = sx; psrc_[1] = sy; psrc_[2] = sz;
     rickerfc_ = rickerfc;
+    drop_graphs();
     return CGFDM_OK;
   }
 
@@ -176,6 +192,7 @@ template <typename S> class EngineT : public Engine {
                        bool scaled) override {
     CUDA_TRY(cudaSetDevice(d_.device));
     free_fault();
+    drop_graphs();
     if (npts <= 0) { fault_on_ = false; return CGFDM_OK; }
     const Layout &L = g_.L;
     std::vector<long long> lidx(npts);
@@ -211,13 +228,32 @@ template <typename S> class EngineT : public Engine {
     CUDA_TRY(h2d(fidx_, lidx.data(), sizeof(long long) * npts));
     CUDA_TRY(cudaMalloc(&frate_, sizeof(float) * rr.size()));
     CUDA_TRY(h2d(frate_, rr.data(), sizeof(float) * rr.size()));
-    fnpts_ = npts; fnt_ = nt; fdt_ = dt;
+    // interpolation index and weight of every step (addMoment.cpp:238-264);
+    // the source stops for good at the first step with srcIt + 1 >= nt
+    const int nts = d_.nt > 0 ? d_.nt : 1;
+    std::vector<int> sit(nts, -1);
+    std::vector<float> stw(nts, 0.0f);
+    for (int it = 0; it < d_.nt; ++it) {
+      const float tmpT = (it + 0.0f) * d_.dt;
+      const int srcIt = (int)(tmpT / dt);
+      if (srcIt + 1 >= nt) break;
+      const float t1 = float(srcIt) * dt;
+      sit[it] = srcIt;
+      stw[it] = (tmpT - t1) / dt;
+    }
+    CUDA_TRY(cudaMalloc(&fit_tab_, sizeof(int) * nts));
+    CUDA_TRY(h2d(fit_tab_, sit.data(), sizeof(int) * nts));
+    CUDA_TRY(cudaMalloc(&ftw_tab_, sizeof(float) * nts));
+    CUDA_TRY(h2d(ftw_tab_, stw.data(), sizeof(float) * nts));
+    fnpts_ = npts;
     fault_on_ = true;
+    drop_graphs();
     return CGFDM_OK;
   }
 
   int set_stations(const int32_t *xyz, int nsta) override {
     CUDA_TRY(cudaSetDevice(d_.device));
+    drop_graphs();
     if (sta_xyz_) { cudaFree(sta_xyz_); sta_xyz_ = nullptr; }
     if (sta_wave_) { cudaFree(sta_wave_); sta_wave_ = nullptr; }
     nsta_ = 0;
@@ -248,6 +284,8 @@ template <typename S> class EngineT : public Engine {
       set_error("run past the configured number of steps nt");
       return CGFDM_ERR_ARG;
     }
+    // work queued earlier on another stream (a batch, another caller) first
+    if (last_stream_ && last_stream_ != st) CUDA_TRY(cudaStreamSynchronize(last_stream_));
     last_stream_ = st;
     if (use_stream_ && tile_rows_ == 0) {
       int rc = tune(st);
@@ -258,42 +296,92 @@ template <typename S> class EngineT : public Engine {
     stream_bytes_ = 0.0;
     if (timing_) CUDA_TRY(cudaEventRecord(ev_[0], st));
     for (int s = 0; s < nsteps; ++s) {
-      const int it = it_;
-      // sources add into W once per step before stage 0 (propagate.cpp:145-151)
-      if (point_on_) {
-        float sm = ricker_moment(rickerfc_, it, d_.dt);
-        const float DH3 = d_.dh * d_.dh * d_.dh;
-        const double CsDT = SCALE_OF<S>::cs * (double)d_.dt;
-        CUDA_TRY(launch_point_source<S>(A_, X_, Y_, cjm_, g_.L, psrc_[0], psrc_[1], psrc_[2],
-                                        amp343_, sm, DH3, CsDT, st));
-        ++launches_;
-      }
-      if (fault_on_) {
-        // addMoment.cpp:238-264
-        float tmpT = (it + 0.0f) * d_.dt;
-        int srcIt = (int)(tmpT / fdt_);
-        if (srcIt + 1 >= fnt_) {
-          fault_on_ = false;
-        } else {
-          float t1 = float(srcIt) * fdt_;
-          float tw = (tmpT - t1) / fdt_;
-          CUDA_TRY(launch_fault_source<S>(A_, g_.L.fs, fidx_, frate_, fnpts_, srcIt, tw, d_.dt, st));
-          if (fnpts_ > 0) ++launches_;
+      const int p = it_ % 8;
+      if (use_graph_ && !timing_) {
+        // one step is replayed as a CUDA graph per phase it % 8 (the phase
+        // fixes the MacCormack signs); the first step of a phase runs
+        // eagerly (kernel attributes get set), the second is captured
+        if (!gexec_[p] && gseen_[p]) {
+          int rc = capture_step(st, gexec_[p]);
+          if (rc) return rc;
         }
+        if (gexec_[p]) {
+          CUDA_TRY(cudaGraphLaunch(gexec_[p], st));
+          launches_ += glaunches_[p];
+          ++it_;
+          continue;
+        }
+        gseen_[p] = true;
       }
-      int fb[3] = {kFB[it % 8][0], kFB[it % 8][1], kFB[it % 8][2]};
-      for (int irk = 0; irk < 4; ++irk) {
-        int rc = launch_stage(irk, fb, st);
-        if (rc) return rc;
-        fb[0] = -fb[0]; fb[1] = -fb[1]; fb[2] = -fb[2];
-      }
-      const float c1 = (float)(1.0 / SCALE_OF<S>::cv), c2 = (float)(1.0 / SCALE_OF<S>::cs);
-      CUDA_TRY(launch_station_pgv<S>(A_, g_.L, sta_xyz_, nsta_, d_.nt, it, sta_wave_, pgv_, c1, c2,
-                                     1.0 / SCALE_OF<S>::cv, st));
-      ++launches_;
-      ++it_;
+      const int before = launches_;
+      int rc = eager_step(st);
+      if (rc) return rc;
+      glaunches_[p] = launches_ - before;
     }
     if (timing_) CUDA_TRY(cudaEventRecord(ev_[1], st));
+    return CGFDM_OK;
+  }
+
+  // The pieces of one step: sources into W once before stage 0
+  // (propagate.cpp:145-151), then four stages, then stations / PGV and the
+  // step counter.  The batch runner calls them member by member.
+  int step_sources(cudaStream_t st) {
+    if (point_on_) {
+      const float DH3 = d_.dh * d_.dh * d_.dh;
+      const double CsDT = SCALE_OF<S>::cs * (double)d_.dt;
+      CUDA_TRY(launch_point_source<S>(A_, X_, Y_, cjm_, g_.L, psrc_[0], psrc_[1], psrc_[2],
+                                      amp343_, moment_tab_, step_, DH3, CsDT, st));
+      ++launches_;
+    }
+    if (fault_on_ && fnpts_ > 0) {
+      CUDA_TRY(launch_fault_source<S>(A_, g_.L.fs, fidx_, frate_, fnpts_, fit_tab_, ftw_tab_,
+                                      step_, d_.dt, st));
+      ++launches_;
+    }
+    return CGFDM_OK;
+  }
+
+  int step_end(cudaStream_t st) {
+    const float c1 = (float)(1.0 / SCALE_OF<S>::cv), c2 = (float)(1.0 / SCALE_OF<S>::cs);
+    CUDA_TRY(launch_station_pgv<S>(A_, g_.L, sta_xyz_, nsta_, d_.nt, step_, sta_wave_, pgv_, c1,
+                                   c2, 1.0 / SCALE_OF<S>::cv, st));
+    CUDA_TRY(launch_step_advance(step_, st));
+    launches_ += 2;
+    ++it_;
+    return CGFDM_OK;
+  }
+
+  void step_fb(int irk, int fb[3]) const {
+    const int sg = (irk % 2) ? -1 : 1;  // the signs flip after every stage
+    for (int q = 0; q < 3; ++q) fb[q] = sg * kFB[it_ % 8][q];
+  }
+
+  int eager_step(cudaStream_t st) {
+    int rc = step_sources(st);
+    for (int irk = 0; irk < 4 && !rc; ++irk) {
+      int fb[3];
+      step_fb(irk, fb);
+      rc = launch_stage(irk, fb, st);
+    }
+    return rc ? rc : step_end(st);
+  }
+
+  int capture_step(cudaStream_t st, cudaGraphExec_t &out) {
+    const int it0 = it_, l0 = launches_;
+    CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = eager_step(st);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    it_ = it0;  // nothing ran: the graph replays the step
+    launches_ = l0;
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    CUDA_TRY(e);
+    e = cudaGraphInstantiate(&out, g, 0);
+    cudaGraphDestroy(g);
+    CUDA_TRY(e);
     return CGFDM_OK;
   }
 
@@ -301,6 +389,7 @@ template <typename S> class EngineT : public Engine {
     CUDA_TRY(cudaSetDevice(d_.device));
     cudaStream_t st = stream ? (cudaStream_t)stream : own_stream_;
     int fb[3] = {fb1, fb2, fb3};
+    if (last_stream_ && last_stream_ != st) CUDA_TRY(cudaStreamSynchronize(last_stream_));
     last_stream_ = st;
     return launch_stage(irk, fb, st);
   }
@@ -430,6 +519,13 @@ template <typename S> class EngineT : public Engine {
       return CGFDM_ERR_ARG;
     }
     tile_rows_ = rows;
+    drop_graphs();
+    return CGFDM_OK;
+  }
+
+  int set_graph(bool on) override {
+    use_graph_ = on;
+    drop_graphs();
     return CGFDM_OK;
   }
 
@@ -624,6 +720,20 @@ template <typename S> class EngineT : public Engine {
     return CGFDM_OK;
   }
 
+  // The exact-order kernel on the three free-surface layers of stage irk
+  // (the streaming part of the stage runs in a batch launch).
+  int launch_top(int irk, const int fb[3], cudaStream_t st) {
+    static const int out_of[4] = {1, 2, 1, 0};
+    StageArgs<S> a = stage_args(irk, fb);
+    last_out_ = a.wout;
+    last_aux_out_ = aux_total_ > 0 ? auxbuf(out_of[irk]) : nullptr;
+    a.kbeg = g_.L.nz_ - HALO - 3;
+    a.kend = g_.L.nz_ - HALO;
+    CUDA_TRY(launch_stage_exact<S>(a, st));
+    ++launches_;
+    return CGFDM_OK;
+  }
+
   cudaError_t upload_repacked(const float *src, S *dst, int nfield) {
     float *tmp = nullptr;
     const size_t n = (size_t)nfield * g_.num;
@@ -651,10 +761,20 @@ template <typename S> class EngineT : public Engine {
   }
 
   void free_fault() {
-    if (fidx_) cudaFree(fidx_);
-    if (frate_) cudaFree(frate_);
+    for (void *p : {(void *)fidx_, (void *)frate_, (void *)fit_tab_, (void *)ftw_tab_})
+      if (p) cudaFree(p);
     fidx_ = nullptr;
     frate_ = nullptr;
+    fit_tab_ = nullptr;
+    ftw_tab_ = nullptr;
+  }
+
+  void drop_graphs() {
+    for (int p = 0; p < 8; ++p) {
+      if (gexec_[p]) cudaGraphExecDestroy(gexec_[p]);
+      gexec_[p] = nullptr;
+      gseen_[p] = false;
+    }
   }
 
   void release() {
@@ -663,9 +783,10 @@ template <typename S> class EngineT : public Engine {
     if (last_stream_) cudaStreamSynchronize(last_stream_);
     for (void *p : {(void *)A_, (void *)X_, (void *)Y_, (void *)T_, (void *)cjm_, (void *)rdz_,
                     (void *)pml_, (void *)aux_, (void *)pgv_, (void *)amp343_, (void *)sta_xyz_,
-                    (void *)sta_wave_, (void *)err_flag_})
+                    (void *)sta_wave_, (void *)err_flag_, (void *)step_, (void *)moment_tab_})
       if (p) cudaFree(p);
     free_fault();
+    drop_graphs();
     for (auto &e : ev_)
       if (e) cudaEventDestroy(e);
     for (auto &e : stage_ev_) cudaEventDestroy(e);
@@ -688,8 +809,6 @@ template <typename S> class EngineT : public Engine {
   long long *fidx_ = nullptr;
   float *frate_ = nullptr;
   long long fnpts_ = 0;
-  int fnt_ = 0;
-  float fdt_ = 0;
   int it_ = 0;
   S *last_out_ = nullptr;
   R *last_aux_out_ = nullptr;
@@ -700,6 +819,14 @@ template <typename S> class EngineT : public Engine {
   int stage_used_ = 0;
   int launches_ = 0;          // kernels launched by the last run()
   int tile_rows_ = 0;         // streaming-kernel tile height; 0 = autotune at the first run()
+  int *step_ = nullptr;       // device copy of it_
+  float *moment_tab_ = nullptr;            // point-source moment per step
+  int *fit_tab_ = nullptr;                 // fault interpolation index per step (-1: ended)
+  float *ftw_tab_ = nullptr;               // fault interpolation weight per step
+  bool use_graph_ = false;
+  cudaGraphExec_t gexec_[8] = {};          // one step per phase it % 8
+  bool gseen_[8] = {};
+  int glaunches_[8] = {};                  // kernels in a step of that phase
   double stream_bytes_ = 0;   // algorithmic bytes of its streaming-kernel launches
 };
 
@@ -712,6 +839,218 @@ int64_t engine_device_bytes(const cgfdm_desc &d) {
   int64_t aux = 0;
   for (int q = 0; q < 5; ++q) aux += g.slab_pts[q] * 9;
   return s * (4 * 9 + 13) * g.L.fs + r * (18 * g.nsurf + 4 * aux) + 8 * (int64_t)d.nx * d.ny;
+}
+
+namespace {
+
+// Several handles of one precision advanced together: per step, each
+// member's sources; per stage, the streaming part of all members in
+// persistent launches whose work queue spans them (members grouped by their
+// MacCormack signs, which depend on each member's own step), then each
+// member's free-surface layers; then stations / PGV.  A step can be
+// replayed as a CUDA graph (per phase of the batch's step count mod 8, since
+// every member's signs repeat with period 8).
+template <typename S> class BatchT : public BatchBase {
+ public:
+  explicit BatchT(std::vector<EngineT<S> *> m) : m_(std::move(m)) {}
+  ~BatchT() override {
+    cudaSetDevice(dev_);
+    if (own_) cudaStreamSynchronize(own_);
+    if (last_) cudaStreamSynchronize(last_);
+    for (auto *m : m_)  // the batch's stream goes away with it; its work is done
+      if (m->last_stream_ == own_) m->last_stream_ = nullptr;
+    drop_graphs();
+    if (err_) cudaFree(err_);
+    if (own_) cudaStreamDestroy(own_);
+  }
+
+  int init() {
+    dev_ = m_[0]->d_.device;
+    CUDA_TRY(cudaSetDevice(dev_));
+    CUDA_TRY(cudaStreamCreateWithFlags(&own_, cudaStreamNonBlocking));
+    CUDA_TRY(cudaMalloc(&err_, 2 * sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(err_, 0, 2 * sizeof(int), own_));
+    CUDA_TRY(cudaStreamSynchronize(own_));
+    return CGFDM_OK;
+  }
+
+  int set_graph(bool on) override {
+    use_graph_ = on;
+    drop_graphs();
+    return CGFDM_OK;
+  }
+
+  int run(int nsteps, void *stream) override {
+    CUDA_TRY(cudaSetDevice(dev_));
+    cudaStream_t st = stream ? (cudaStream_t)stream : own_;
+    for (auto *m : m_)
+      if (m->it_ + nsteps > m->d_.nt) {
+        set_error("batch run past a member's configured number of steps nt");
+        return CGFDM_ERR_ARG;
+      }
+    last_ = st;
+    for (auto *m : m_) {
+      // members' own work (uploads, earlier runs) comes first on this stream
+      if (m->last_stream_ && m->last_stream_ != st) CUDA_TRY(cudaStreamSynchronize(m->last_stream_));
+      CUDA_TRY(cudaStreamSynchronize(m->own_stream_));
+      m->last_stream_ = st;
+    }
+    for (int s = 0; s < nsteps; ++s) {
+      const int p = count_ % 8;
+      if (use_graph_) {
+        if (!gexec_[p] && gseen_[p]) {
+          int rc = capture_step(st, gexec_[p]);
+          if (rc) return rc;
+        }
+        if (gexec_[p]) {
+          CUDA_TRY(cudaGraphLaunch(gexec_[p], st));
+          for (auto *m : m_) ++m->it_;
+          ++count_;
+          continue;
+        }
+        gseen_[p] = true;
+      }
+      int rc = eager_step(st);
+      if (rc) return rc;
+      ++count_;
+    }
+    return CGFDM_OK;
+  }
+
+  int synchronize() override {
+    CUDA_TRY(cudaSetDevice(dev_));
+    if (last_) CUDA_TRY(cudaStreamSynchronize(last_));
+    int flag = 0;
+    CUDA_TRY(cudaMemcpy(&flag, err_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+      set_error("a bounded device-side wait of the streaming kernel expired");
+      return CGFDM_ERR_TIMEOUT;
+    }
+    return CGFDM_OK;
+  }
+
+ private:
+  int eager_step(cudaStream_t st) {
+    static const int in_of[4] = {0, 1, 2, 1};
+    for (auto *m : m_) {
+      int rc = m->step_sources(st);
+      if (rc) return rc;
+    }
+    std::vector<StageArgs<S>> args;
+    std::vector<const void *> maps;
+    for (int irk = 0; irk < 4; ++irk) {
+      for (int code = 0; code < 8; ++code) {
+        args.clear();
+        maps.clear();
+        for (auto *m : m_) {
+          int fb[3];
+          m->step_fb(irk, fb);
+          if (!m->use_stream_ || (fb[0] > 0) * 4 + (fb[1] > 0) * 2 + (fb[2] > 0) != code) continue;
+          StageArgs<S> a = m->stage_args(irk, fb);
+          a.kbeg = HALO;
+          a.kend = m->g_.L.nz_ - HALO - 3;
+          args.push_back(a);
+          maps.push_back(m->tmap_[in_of[irk]]);
+        }
+        if (!args.empty())
+          CUDA_TRY(launch_stage_stream_batch<S>(args.data(), maps.data(), (int)args.size(), err_,
+                                                err_ + 1, st));
+      }
+      for (auto *m : m_) {
+        int fb[3];
+        m->step_fb(irk, fb);
+        int rc = m->use_stream_ ? m->launch_top(irk, fb, st) : m->launch_stage(irk, fb, st);
+        if (rc) return rc;
+      }
+    }
+    for (auto *m : m_) {
+      int rc = m->step_end(st);
+      if (rc) return rc;
+    }
+    return CGFDM_OK;
+  }
+
+  int capture_step(cudaStream_t st, cudaGraphExec_t &out) {
+    std::vector<int> it0, l0;
+    for (auto *m : m_) {
+      it0.push_back(m->it_);
+      l0.push_back(m->launches_);
+    }
+    CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = eager_step(st);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    for (size_t q = 0; q < m_.size(); ++q) {  // nothing ran: the graph replays the step
+      m_[q]->it_ = it0[q];
+      m_[q]->launches_ = l0[q];
+    }
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    CUDA_TRY(e);
+    e = cudaGraphInstantiate(&out, g, 0);
+    cudaGraphDestroy(g);
+    CUDA_TRY(e);
+    return CGFDM_OK;
+  }
+
+  void drop_graphs() {
+    for (int p = 0; p < 8; ++p) {
+      if (gexec_[p]) cudaGraphExecDestroy(gexec_[p]);
+      gexec_[p] = nullptr;
+      gseen_[p] = false;
+    }
+  }
+
+  std::vector<EngineT<S> *> m_;
+  int dev_ = 0;
+  cudaStream_t own_ = nullptr, last_ = nullptr;
+  int *err_ = nullptr;  // [0] error flag, [1] work counter of the batched launches
+  bool use_graph_ = false;
+  cudaGraphExec_t gexec_[8] = {};
+  bool gseen_[8] = {};
+  long long count_ = 0;  // steps run by this batch
+};
+
+template <typename S>
+int make_batch_t(Engine *const *members, int n, std::unique_ptr<BatchBase> &out) {
+  std::vector<EngineT<S> *> m;
+  for (int q = 0; q < n; ++q) {
+    auto *e = dynamic_cast<EngineT<S> *>(members[q]);
+    if (!e) {
+      set_error("batch members must share one precision");
+      return CGFDM_ERR_ARG;
+    }
+    for (auto *o : m)
+      if (o == e) {
+        set_error("a handle appears twice in the batch");
+        return CGFDM_ERR_ARG;
+      }
+    if (!m.empty() && e->desc().device != m[0]->desc().device) {
+      set_error("batch members must share one device");
+      return CGFDM_ERR_ARG;
+    }
+    m.push_back(e);
+  }
+  auto *b = new BatchT<S>(std::move(m));
+  out.reset(b);
+  return b->init();
+}
+
+}  // namespace
+
+int make_batch(Engine *const *members, int n, std::unique_ptr<BatchBase> &out) {
+  if (!members || n <= 0) {
+    set_error("empty batch");
+    return CGFDM_ERR_ARG;
+  }
+  switch (members[0]->desc().precision) {
+    case CGFDM_FP32: return make_batch_t<float>(members, n, out);
+    case CGFDM_FP16: return make_batch_t<__half>(members, n, out);
+    case CGFDM_BF16: return make_batch_t<__nv_bfloat16>(members, n, out);
+    default: return make_batch_t<double>(members, n, out);
+  }
 }
 
 int make_engine(const cgfdm_desc &d, std::unique_ptr<Engine> &out) {

@@ -38,11 +38,23 @@ class Engine {
   virtual int get_timing(float *ms3) = 0;
   virtual int get_kernel_stats(double *out8) = 0;
   virtual int set_tile_rows(int rows) = 0;
+  virtual int set_graph(bool on) = 0;
   virtual const cgfdm_desc &desc() const = 0;
+};
+
+// Several handles of one precision and device advanced together with
+// batched streaming launches (see BatchT in engine.cu).
+class BatchBase {
+ public:
+  virtual ~BatchBase() = default;
+  virtual int run(int nsteps, void *stream) = 0;
+  virtual int set_graph(bool on) = 0;
+  virtual int synchronize() = 0;
 };
 
 // Creates the engine for desc->precision; returns a status code.
 int make_engine(const cgfdm_desc &desc, std::unique_ptr<Engine> &out);
+int make_batch(Engine *const *members, int n, std::unique_ptr<BatchBase> &out);
 int64_t engine_device_bytes(const cgfdm_desc &desc);
 
 // PML profiles of init_pml_para.cpp:99-234 for a single rank with the free

@@ -32,6 +32,14 @@ cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps, int *er
                                 int *work_counter, cudaStream_t st,
                                 cudaEvent_t after_main = nullptr, int *nlaunch = nullptr,
                                 int tile_rows = 16);
+// One stage (same irk and MacCormack signs for all) of n scenarios in
+// persistent launches whose work queue spans all of them (16 scenarios per
+// launch pair); maps[q] is scenario q's encode_stream_maps buffer.  Tile
+// height 16.
+template <typename S>
+cudaError_t launch_stage_stream_batch(const StageArgs<S> *args, const void *const *maps, int n,
+                                      int *err_flag, int *work_counter, cudaStream_t st,
+                                      int *nlaunch = nullptr);
 template <typename S> bool stage_stream_supported();
 // Encodes the tensor maps the streaming kernel loads its tiles through (the
 // 9 wavefield components of the stage input `wave`, the 13 coefficient
@@ -41,25 +49,36 @@ template <typename S>
 int encode_stream_maps(const S *wave, const S *cjm, const S *wm, const S *t, const Layout &L,
                        void *out);
 
-// Smoothed point source (singleSource.cpp:78-127): adds value(cell) to
-// Txx, Tyy, Tzz of w0 and, for cells in the halo, of w1 and w2 too (halo
-// cells hold constant values that every stage buffer must share).
+// Per-step values come from device memory so that a step can be replayed as
+// a CUDA graph: `step` points at the device step counter, advanced by
+// launch_step_advance at the end of every step.
+
+// Smoothed point source (singleSource.cpp:78-127) with the source moment
+// moment[*step]: adds value(cell) to Txx, Tyy, Tzz of w0 and, for cells in
+// the halo, of w1 and w2 too (halo cells hold constant values that every
+// stage buffer must share).
 template <typename S>
 cudaError_t launch_point_source(S *w0, S *w1, S *w2, const S *cjm, Layout L, int sx, int sy,
-                                int sz, const float *amp343, float s, float DH3, double CsDT,
-                                cudaStream_t st);
+                                int sz, const float *amp343, const float *moment, const int *step,
+                                float DH3, double CsDT, cudaStream_t st);
 
-// Finite-fault injection (addMoment.cpp:98-219, NO_SOURCE_SMOOTH); idx are
-// offsets in the HBM layout.
+// Finite-fault injection (addMoment.cpp:98-219, NO_SOURCE_SMOOTH) at the
+// interpolation index src_it[*step] (negative: the source has ended) and
+// weight src_tw[*step]; idx are offsets in the HBM layout.
 template <typename S>
 cudaError_t launch_fault_source(S *w, long long fs, const long long *idx, const float *rate,
-                                long long npts, int srcIt, float tw, float DT, cudaStream_t st);
+                                long long npts, const int *src_it, const float *src_tw,
+                                const int *step, float DT, cudaStream_t st);
 
-// Station sampling (station.cpp:310-347) and PGV (PGV.cpp:49-101).
+// Station sampling (station.cpp:310-347) and PGV (PGV.cpp:49-101) of step
+// *step.
 template <typename S>
-cudaError_t launch_station_pgv(const S *w, Layout L, const int *xyz, int nsta, int NT, int it,
-                               float *wave, float *pgv, float c1, float c2, double cv_inv,
-                               cudaStream_t st);
+cudaError_t launch_station_pgv(const S *w, Layout L, const int *xyz, int nsta, int NT,
+                               const int *step, float *wave, float *pgv, float c1, float c2,
+                               double cv_inv, cudaStream_t st);
+
+// ++*step (one thread).
+cudaError_t launch_step_advance(int *step, cudaStream_t st);
 
 // One field's interior slice at padded index `at` along axis 0/1/2, times
 // c (data_io.cpp:86-231).

@@ -36,6 +36,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <type_traits>
 
@@ -314,10 +315,52 @@ __device__ __forceinline__ void item_of(const Work &w, int item, int &bxi, int &
   }
 }
 
-template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK>
-__global__ void __launch_bounds__(TX * TYv, Geo<S, TYv>::MINB)
-    stage_stream_kernel(const __grid_constant__ Maps maps, const StageArgs<S> a, const Work wk,
-                        int *err) {
+// Where the work items of a launch come from: one scenario (SingleSrc) or
+// up to kBatchMax scenarios of one batch (BatchSrc), each with its own stage
+// arguments, tensor maps and item geometry; the items of a batch are numbered
+// scenario after scenario.
+template <typename S> struct SingleSrc {
+  const Maps &m;
+  const StageArgs<S> &a;
+  const Work &w;
+  __device__ int *counter() const { return w.counter; }
+  __device__ int nitems() const { return w.nitems; }
+  __device__ int entry_of(int item, int &local) const {
+    local = item;
+    return 0;
+  }
+  __device__ const StageArgs<S> &args(int) const { return a; }
+  __device__ const Maps &maps(int) const { return m; }
+  __device__ const Work &work(int) const { return w; }
+};
+
+constexpr int kBatchMax = 16;
+template <typename S> struct BatchParams {
+  Maps maps[kBatchMax];
+  StageArgs<S> args[kBatchMax];
+  Work work[kBatchMax];
+  int item_end[kBatchMax];  // items of scenarios 0..e together
+  int n;
+  int *counter;
+};
+
+template <typename S> struct BatchSrc {
+  const BatchParams<S> &p;
+  __device__ int *counter() const { return p.counter; }
+  __device__ int nitems() const { return p.item_end[p.n - 1]; }
+  __device__ int entry_of(int item, int &local) const {
+    int e = 0;
+    while (e + 1 < p.n && item >= p.item_end[e]) ++e;
+    local = item - (e ? p.item_end[e - 1] : 0);
+    return e;
+  }
+  __device__ const StageArgs<S> &args(int e) const { return p.args[e]; }
+  __device__ const Maps &maps(int e) const { return p.maps[e]; }
+  __device__ const Work &work(int e) const { return p.work[e]; }
+};
+
+template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK, typename Src>
+__device__ __forceinline__ void stream_body(const Src &src, int *err) {
   using G = Geo<S, TYv>;
   constexpr int TY = G::TY, NTHR = G::NTHR, BY = G::BY;
   constexpr int NW = G::NW, NC = G::NC, NM = G::NM, BX = G::BX;
@@ -331,17 +374,6 @@ __global__ void __launch_bounds__(TX * TYv, Geo<S, TYv>::MINB)
 
   const int tid = threadIdx.x;
   const int c = tid % TX, r = tid / TX;
-  const Layout L = a.L;
-  const int irk = a.irk;
-  const bool need_m = irk == 1 || irk == 2, need_t = irk >= 1;
-  const uint32_t m_bytes = (need_m ? 9 : 0) * NTHR * G::ES + (need_t ? 9 : 0) * NTHR * G::ES;
-  const float rDH = a.rDH, DT = a.DT;
-  // stencil weights with the MacCormack sign and 1/DH folded in
-  const float wx[5] = {FB1 * kAm1 * rDH, FB1 * kA0 * rDH, FB1 * kA1 * rDH, FB1 * kA2 * rDH, FB1 * kA3 * rDH};
-  const float wy[5] = {FB2 * kAm1 * rDH, FB2 * kA0 * rDH, FB2 * kA1 * rDH, FB2 * kA2 * rDH, FB2 * kA3 * rDH};
-  const float wz[5] = {FB3 * kAm1 * rDH, FB3 * kA0 * rDH, FB3 * kA1 * rDH, FB3 * kA2 * rDH, FB3 * kA3 * rDH};
-  const float *px = a.pml, *py = a.pml + 3 * L.nx_, *pz = a.pml + 3 * L.nx_ + 3 * L.ny_;
-  const long long fs = L.fs;
   const int cidx = r * TX + c;
 
   if (tid == 0) {
@@ -355,12 +387,28 @@ __global__ void __launch_bounds__(TX * TYv, Geo<S, TYv>::MINB)
   unsigned fw0 = 0, fc0 = 0, fm0 = 0;
 
   for (;;) {
-    if (tid == 0) s_item = atomicAdd(wk.counter, 1);
+    if (tid == 0) s_item = atomicAdd(src.counter(), 1);
     __syncthreads();
     const int item = s_item;
-    if (item >= wk.nitems || s_bad) break;
+    if (item >= src.nitems() || s_bad) break;
+    int local;
+    const int e = src.entry_of(item, local);
+    const StageArgs<S> &a = src.args(e);
+    const Maps &maps = src.maps(e);
+    const Work &wk = src.work(e);
+    const Layout L = a.L;
+    const int irk = a.irk;
+    const bool need_m = irk == 1 || irk == 2, need_t = irk >= 1;
+    const uint32_t m_bytes = (need_m ? 9 : 0) * NTHR * G::ES + (need_t ? 9 : 0) * NTHR * G::ES;
+    const float rDH = a.rDH, DT = a.DT;
+    // stencil weights with the MacCormack sign and 1/DH folded in
+    const float wx[5] = {FB1 * kAm1 * rDH, FB1 * kA0 * rDH, FB1 * kA1 * rDH, FB1 * kA2 * rDH, FB1 * kA3 * rDH};
+    const float wy[5] = {FB2 * kAm1 * rDH, FB2 * kA0 * rDH, FB2 * kA1 * rDH, FB2 * kA2 * rDH, FB2 * kA3 * rDH};
+    const float wz[5] = {FB3 * kAm1 * rDH, FB3 * kA0 * rDH, FB3 * kA1 * rDH, FB3 * kA2 * rDH, FB3 * kA3 * rDH};
+    const float *px = a.pml, *py = a.pml + 3 * L.nx_, *pz = a.pml + 3 * L.nx_ + 3 * L.ny_;
+    const long long fs = L.fs;
     int bxi, byi, kb, ke;
-    item_of<PMLK>(wk, item, bxi, byi, kb, ke, a.kbeg, a.kend);
+    item_of<PMLK>(wk, local, bxi, byi, kb, ke, a.kbeg, a.kend);
     const int nout = ke - kb, nplanes = nout + 4;
     const int q0 = DIR > 0 ? kb - 3 : ke + 2;  // input planes q_n = q0 + n*DIR
     const int i = HALO + bxi * TX + c, j = HALO + byi * TY + r;
@@ -586,6 +634,19 @@ __global__ void __launch_bounds__(TX * TYv, Geo<S, TYv>::MINB)
 }
 
 template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK>
+__global__ void __launch_bounds__(TX * TYv, Geo<S, TYv>::MINB)
+    stage_stream_kernel(const __grid_constant__ Maps maps, const __grid_constant__ StageArgs<S> a,
+                        const __grid_constant__ Work wk, int *err) {
+  stream_body<S, TYv, FB1, FB2, FB3, PMLK>(SingleSrc<S>{maps, a, wk}, err);
+}
+
+template <typename S, int FB1, int FB2, int FB3, bool PMLK>
+__global__ void __launch_bounds__(TX * 16, 1)
+    stage_stream_batch_kernel(const __grid_constant__ BatchParams<S> p, int *err) {
+  stream_body<S, 16, FB1, FB2, FB3, PMLK>(BatchSrc<S>{p}, err);
+}
+
+template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK>
 cudaError_t launch_variant(const StageArgs<S> &a, const Maps &maps, const Work &wk, int *err,
                            int nsm, cudaStream_t st) {
   using G = Geo<S, TYv>;
@@ -606,13 +667,7 @@ cudaError_t launch_variant(const StageArgs<S> &a, const Maps &maps, const Work &
   return cudaGetLastError();
 }
 
-// Splits the stage into the interior launch (tiles and chunks that touch no
-// PML slab) and the PML launch (the rest), see Work.
-template <typename S, int TYv, int FB1, int FB2, int FB3>
-cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *counter,
-                       cudaStream_t st, int *nlaunch) {
-  constexpr int TY = TYv;
-  constexpr int slots = Geo<S, TYv>::MINB;  // CTAs resident per SM
+int sm_count() {
   static int nsm = 0;
   if (!nsm) {
     int dev = 0;
@@ -620,6 +675,19 @@ cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *c
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (nsm <= 0) nsm = 148;
   }
+  return nsm;
+}
+
+// Item geometry of one stage of one scenario (see Work) and the item counts
+// of its interior and PML launches.
+struct WorkPlan {
+  Work wk;
+  int n_in, n_pml;
+};
+template <typename S, int TYv>
+WorkPlan plan_work(const StageArgs<S> &a, int nsm, int *counter) {
+  constexpr int TY = TYv;
+  constexpr int slots = Geo<S, TYv>::MINB;  // CTAs resident per SM
   const int nx = a.L.nx_ - 2 * HALO, ny = a.L.ny_ - 2 * HALO;
   const int np = a.nslab ? a.npml : 0;
   Work wk;
@@ -647,20 +715,94 @@ cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *c
   if (pl_i > 0) nic = std::max(1, std::min(nic, pl_i / 24));
   wk.chunk_i = nic ? (pl_i + nic - 1) / nic : 1;
   wk.nic = nic ? (pl_i + wk.chunk_i - 1) / wk.chunk_i : 0;
+  wk.nitems = 0;
+  return {wk, tiles_in * wk.nic, wk.nzc * tiles + (tiles - tiles_in) * wk.nic};
+}
+
+// Splits the stage into the interior launch (tiles and chunks that touch no
+// PML slab) and the PML launch (the rest), see Work.
+template <typename S, int TYv, int FB1, int FB2, int FB3>
+cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *counter,
+                       cudaStream_t st, int *nlaunch) {
+  const int nsm = sm_count();
+  const WorkPlan wp = plan_work<S, TYv>(a, nsm, counter);
   cudaError_t e = cudaSuccess;
-  Work wi = wk;
-  wi.nitems = tiles_in * wk.nic;
+  Work wi = wp.wk;
+  wi.nitems = wp.n_in;
   if (wi.nitems > 0) {
     e = launch_variant<S, TYv, FB1, FB2, FB3, false>(a, maps, wi, err, nsm, st);
     if (e != cudaSuccess) return e;
     if (nlaunch) ++*nlaunch;
   }
-  Work wp = wk;
-  wp.nitems = wk.nzc * tiles + (tiles - tiles_in) * wk.nic;
-  if (wp.nitems > 0) {
-    e = launch_variant<S, TYv, FB1, FB2, FB3, true>(a, maps, wp, err, nsm, st);
+  Work wq = wp.wk;
+  wq.nitems = wp.n_pml;
+  if (wq.nitems > 0) {
+    e = launch_variant<S, TYv, FB1, FB2, FB3, true>(a, maps, wq, err, nsm, st);
     if (e != cudaSuccess) return e;
     if (nlaunch) ++*nlaunch;
+  }
+  return cudaSuccess;
+}
+
+template <typename S, int FB1, int FB2, int FB3, bool PMLK>
+cudaError_t launch_batch_variant(const BatchParams<S> &p, int items, int *err, int nsm,
+                                 cudaStream_t st) {
+  using G = Geo<S, 16>;
+  static_assert(sizeof(BatchParams<S>) <= 32000, "kernel parameter space");
+  static int attr_dev = -1;
+  auto kern = stage_stream_batch_kernel<S, FB1, FB2, FB3, PMLK>;
+  const int smem = PMLK ? G::SMEM_P : G::SMEM;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    cudaError_t e =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    attr_dev = dev;
+  }
+  cudaError_t e = cudaMemsetAsync(p.counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  kern<<<std::min(items, nsm), G::NTHR, smem, st>>>(p, err);
+  return cudaGetLastError();
+}
+
+// One stage of n scenarios that share the MacCormack signs: kBatchMax
+// scenarios per launch pair (interior items of all of them, then PML items).
+template <typename S, int FB1, int FB2, int FB3>
+cudaError_t launch_batch(const StageArgs<S> *args, const void *const *maps, int n, int *err,
+                         int *counter, cudaStream_t st, int *nlaunch) {
+  const int nsm = sm_count();
+  // the launch parameters (about 19 KB) are assembled in per-thread storage
+  static thread_local BatchParams<S> params;
+  BatchParams<S> *bp = &params;
+  for (int b0 = 0; b0 < n; b0 += kBatchMax) {
+    const int nb = std::min(kBatchMax, n - b0);
+    for (int pass = 0; pass < 2; ++pass) {
+      std::memset((void *)bp, 0, sizeof(BatchParams<S>));
+      int total = 0, m = 0;
+      for (int q = 0; q < nb; ++q) {
+        const StageArgs<S> &a = args[b0 + q];
+        if (a.kend <= a.kbeg) continue;
+        const WorkPlan wp = plan_work<S, 16>(a, nsm, counter);
+        const int cnt = pass == 0 ? wp.n_in : wp.n_pml;
+        if (cnt <= 0) continue;
+        bp->maps[m] = ((const MapSet *)maps[b0 + q])->ty16;
+        bp->args[m] = a;
+        bp->work[m] = wp.wk;
+        bp->work[m].nitems = cnt;
+        total += cnt;
+        bp->item_end[m] = total;
+        ++m;
+      }
+      if (!m) continue;
+      bp->n = m;
+      bp->counter = counter;
+      cudaError_t e = pass == 0
+                          ? launch_batch_variant<S, FB1, FB2, FB3, false>(*bp, total, err, nsm, st)
+                          : launch_batch_variant<S, FB1, FB2, FB3, true>(*bp, total, err, nsm, st);
+      if (e != cudaSuccess) return e;
+      if (nlaunch) ++*nlaunch;
+    }
   }
   return cudaSuccess;
 }
@@ -761,18 +903,56 @@ cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps_in, int 
                                 int tile_rows) {
   if (a.kend <= a.kbeg) return cudaSuccess;
   const MapSet &ms = *(const MapSet *)maps_in;
-  cudaError_t e = tile_rows == 8 ? launch_fb<S, 8>(a, ms.ty8, err, counter, st, nlaunch)
-                                 : launch_fb<S, 16>(a, ms.ty16, err, counter, st, nlaunch);
+  // tile height 16 runs the batched kernel as a batch of one, so that a
+  // scenario gives the same bits alone and inside a batch
+  cudaError_t e = tile_rows == 8
+                      ? launch_fb<S, 8>(a, ms.ty8, err, counter, st, nlaunch)
+                      : launch_stage_stream_batch<S>(&a, &maps_in, 1, err, counter, st, nlaunch);
   if (e != cudaSuccess) return e;
   if (after_main) e = cudaEventRecord(after_main, st);
   return e;
 }
+template <typename S>
+cudaError_t launch_stage_stream_batch(const StageArgs<S> *args, const void *const *maps, int n,
+                                      int *err, int *counter, cudaStream_t st, int *nlaunch) {
+  if (n <= 0) return cudaSuccess;
+  for (int q = 1; q < n; ++q)
+    if (args[q].fb1 != args[0].fb1 || args[q].fb2 != args[0].fb2 || args[q].fb3 != args[0].fb3 ||
+        args[q].irk != args[0].irk)
+      return cudaErrorInvalidValue;
+  const StageArgs<S> &a = args[0];
+  switch ((a.fb1 > 0) * 4 + (a.fb2 > 0) * 2 + (a.fb3 > 0)) {
+    case 0: return launch_batch<S, -1, -1, -1>(args, maps, n, err, counter, st, nlaunch);
+    case 1: return launch_batch<S, -1, -1, 1>(args, maps, n, err, counter, st, nlaunch);
+    case 2: return launch_batch<S, -1, 1, -1>(args, maps, n, err, counter, st, nlaunch);
+    case 3: return launch_batch<S, -1, 1, 1>(args, maps, n, err, counter, st, nlaunch);
+    case 4: return launch_batch<S, 1, -1, -1>(args, maps, n, err, counter, st, nlaunch);
+    case 5: return launch_batch<S, 1, -1, 1>(args, maps, n, err, counter, st, nlaunch);
+    case 6: return launch_batch<S, 1, 1, -1>(args, maps, n, err, counter, st, nlaunch);
+    default: return launch_batch<S, 1, 1, 1>(args, maps, n, err, counter, st, nlaunch);
+  }
+}
+template <>
+cudaError_t launch_stage_stream_batch<double>(const StageArgs<double> *, const void *const *, int,
+                                              int *, int *, cudaStream_t, int *) {
+  return cudaErrorNotSupported;
+}
+
 template <>
 cudaError_t launch_stage_stream<double>(const StageArgs<double> &, const void *, int *, int *,
                                         cudaStream_t, cudaEvent_t, int *, int) {
   return cudaErrorNotSupported;
 }
 
+template cudaError_t launch_stage_stream_batch<float>(const StageArgs<float> *,
+                                                      const void *const *, int, int *, int *,
+                                                      cudaStream_t, int *);
+template cudaError_t launch_stage_stream_batch<__half>(const StageArgs<__half> *,
+                                                       const void *const *, int, int *, int *,
+                                                       cudaStream_t, int *);
+template cudaError_t launch_stage_stream_batch<__nv_bfloat16>(const StageArgs<__nv_bfloat16> *,
+                                                              const void *const *, int, int *,
+                                                              int *, cudaStream_t, int *);
 template bool stage_stream_supported<float>();
 template bool stage_stream_supported<__half>();
 template bool stage_stream_supported<__nv_bfloat16>();

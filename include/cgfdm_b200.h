@@ -171,6 +171,35 @@ int cgfdm_get_kernel_stats(cgfdm_handle *h, double *out8);
  * choice is cached per (precision, grid) for the process. */
 int cgfdm_set_tile_rows(cgfdm_handle *h, int32_t rows);
 
+/* Replays each time step of cgfdm_run as a CUDA graph (on = 1) instead of
+ * launching its kernels one by one; one graph per phase of the step counter
+ * mod 8 (the MacCormack signs repeat with period 8), captured on the second
+ * step of that phase and kept until the sources, stations, model or tile
+ * height change.  Results are identical either way.  While timing is
+ * enabled (cgfdm_set_timing) steps run without graphs.  The stream passed to
+ * cgfdm_run must be capturable (not the legacy NULL stream: pass NULL to use
+ * the handle's own stream). */
+int cgfdm_set_graph(cgfdm_handle *h, int32_t on);
+
+/* ---- batches: many independent scenarios advanced together ------------
+ * No counterpart in the reference (one run per process there).  A batch
+ * holds n handles of one precision on one device (uneven grid sizes, own
+ * sources, stations, and step counters).  cgfdm_batch_run advances every
+ * member by nsteps: per stage, the streaming part of all members runs in
+ * persistent launches whose work queue spans the members (16 members per
+ * launch pair; members at different phases of the MacCormack schedule are
+ * grouped), and each member's free-surface layers, sources and stations run
+ * as its own small kernels.  Results equal running each member alone.  With
+ * cgfdm_batch_set_graph(b, 1) each batch step is replayed as a CUDA graph.
+ * Members keep their own state: read their results with the handle getters
+ * after cgfdm_batch_synchronize.  Destroy the batch before its members. */
+typedef struct cgfdm_batch cgfdm_batch;
+int cgfdm_batch_create(cgfdm_handle *const *handles, int32_t n, cgfdm_batch **out);
+int cgfdm_batch_run(cgfdm_batch *b, int32_t nsteps, void *stream);
+int cgfdm_batch_set_graph(cgfdm_batch *b, int32_t on);
+int cgfdm_batch_synchronize(cgfdm_batch *b);
+int cgfdm_batch_destroy(cgfdm_batch *b);
+
 /* ---- one RK stage without any device allocation ------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * while they run -- a serving process that splits all of HBM into fixed pools
