@@ -15,6 +15,7 @@ ERR = {1: "ARG", 100: "PARAMS", 110: "CFL", 130: "PML", 180: "NO_SOURCE", 181: "
        200: "IO", 300: "CUDA", 301: "NOMEM", 302: "NO_KERNEL", 303: "TIMEOUT", 304: "STATE"}
 FP32, FP16, BF16, FP64 = 0, 1, 2, 3
 KERNEL_AUTO, KERNEL_EXACT, KERNEL_STREAM = 0, 1, 2
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 
 class CgfdmError(RuntimeError):
@@ -52,6 +53,11 @@ class StageBuffers(C.Structure):
                 ("aux_t", C.c_void_p)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_int64), ("chunk_steps", C.c_int32),
+                ("device", C.c_int32), ("use_graph", C.c_int32)]
+
+
 _lib = None
 
 # name -> (restype, argtypes); every entry point returns int unless noted
@@ -87,6 +93,14 @@ SIGNATURES = {
     "cgfdm_batch_set_graph": (C.c_int, [P, I32]),
     "cgfdm_batch_synchronize": (C.c_int, [P]),
     "cgfdm_batch_destroy": (C.c_int, [P]),
+    "cgfdm_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(P)]),
+    "cgfdm_server_submit": (C.c_int, [P, C.POINTER(Desc), P, P, I32, P, F, P, P, I64, I32, F, P,
+                                      I32, C.POINTER(I64)]),
+    "cgfdm_server_poll": (C.c_int, [P, I64, C.POINTER(I32), C.POINTER(I32)]),
+    "cgfdm_server_read_rows": (C.c_int, [P, I64, I32, P, C.POINTER(I32)]),
+    "cgfdm_server_wait": (C.c_int, [P, I64, P, P, P]),
+    "cgfdm_server_stats": (C.c_int, [P, P]),
+    "cgfdm_server_destroy": (C.c_int, [P]),
     "cgfdm_propagate": (C.c_int, [C.POINTER(Desc), P, P, I32, P, F, P, P, I64, I32, F, P, I32,
                                   P, P, P]),
     "cgfdm_run_directory": (C.c_int, [C.c_char_p, I32, I32, I32]),

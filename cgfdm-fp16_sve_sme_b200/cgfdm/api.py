@@ -203,6 +203,83 @@ class Batch:
         self.close()
 
 
+class Server:
+    """The library's request loop with continuous batching (cgfdm_server_*).
+
+    submit() queues a simulation and returns its id at once; the server's
+    worker admits requests by free HBM, advances all admitted requests of a
+    precision as one batch, and streams seismogram rows back every `chunk`
+    steps.  wait(id) returns (seismograms, pgv, (ms to first chunk, ms to
+    completion))."""
+
+    def __init__(self, hbm_budget_bytes=0, chunk=100, device=0, graph=True):
+        o = _lib.ServerOpts(int(hbm_budget_bytes), int(chunk), int(device), int(graph))
+        sv = C.c_void_p()
+        check(lib().cgfdm_server_create(C.byref(o), C.byref(sv)))
+        self._s = sv
+        self._shape = {}
+
+    def submit(self, desc, cjm, rdz, *, point=None, rickerfc=0.0, src_index=None,
+               moment_rate=None, src_nt=0, src_dt=0.0, stations=None):
+        cjm, rdz = _f32(cjm), _f32(rdz)
+        pxyz = None if point is None else np.ascontiguousarray(point, np.int32)
+        idx = None if src_index is None else np.ascontiguousarray(src_index, np.int64)
+        mr = _f32(moment_rate)
+        sta = None if stations is None else np.ascontiguousarray(stations, np.int32).reshape(-1, 3)
+        nsta = 0 if sta is None else len(sta)
+        rid = C.c_int64()
+        check(lib().cgfdm_server_submit(
+            self._s, C.byref(desc), _ptr(cjm), _ptr(rdz), int(point is not None), _ptr(pxyz),
+            np.float32(rickerfc), _ptr(idx), _ptr(mr), 0 if idx is None else idx.size, src_nt,
+            np.float32(src_dt), _ptr(sta), nsta, C.byref(rid)))
+        self._shape[rid.value] = (nsta, desc.nt, desc.ny, desc.nx)
+        return rid.value
+
+    def poll(self, rid):
+        st, steps = C.c_int32(), C.c_int32()
+        check(lib().cgfdm_server_poll(self._s, rid, C.byref(st), C.byref(steps)))
+        return st.value, steps.value
+
+    def read_rows(self, rid, out, start=0):
+        """Copies the rows streamed back so far (from `start`) into out
+        ([nsta][nt][9] float32); returns the row count available."""
+        upto = C.c_int32()
+        check(lib().cgfdm_server_read_rows(self._s, rid, start, _ptr(out), C.byref(upto)))
+        return upto.value
+
+    def wait(self, rid):
+        nsta, nt, ny, nx = self._shape.pop(rid)
+        wave = np.zeros((nsta, nt, 9), np.float32)
+        pgv = np.zeros((ny, nx, 2), np.float32)
+        lat = np.zeros(2, np.float64)
+        check(lib().cgfdm_server_wait(self._s, rid, _ptr(wave), _ptr(pgv), _ptr(lat)))
+        return wave, pgv, (float(lat[0]), float(lat[1]))
+
+    def stats(self):
+        v = np.zeros(8, np.float64)
+        check(lib().cgfdm_server_stats(self._s, _ptr(v)))
+        return {"first_p50_ms": v[0], "first_p99_ms": v[1], "done_p50_ms": v[2],
+                "done_p99_ms": v[3], "gpts": v[4], "completed": int(v[5]), "busy_s": v[6],
+                "peak_bytes": v[7]}
+
+    def close(self):
+        if getattr(self, "_s", None):
+            lib().cgfdm_server_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 def propagate(desc, cjm, rdz, *, point=None, rickerfc=0.0, src_index=None, moment_rate=None,
               src_nt=0, src_dt=0.0, stations=None):
     """propagate() drop-in with host buffers; returns (stations, pgv, free_surface)."""
@@ -297,5 +374,5 @@ def run_directory(run_dir, precision=_lib.FP32, kernel=_lib.KERNEL_AUTO, device=
     check(lib().cgfdm_run_directory(run_dir.encode(), precision, kernel, device))
 
 
-__all__ = ["Simulation", "Batch", "propagate", "setup_from_directory", "run_directory", "make_desc",
+__all__ = ["Simulation", "Batch", "Server", "propagate", "setup_from_directory", "run_directory", "make_desc",
            "device_bytes", "CgfdmError", "hbm_layout", "stage_noalloc"]

@@ -418,6 +418,23 @@ template <typename S> class EngineT : public Engine {
     return CGFDM_OK;
   }
 
+  int get_station_rows(float *wave, int it0, int it1) override {
+    // rows [it0, it1) of every station into the same places of a host
+    // [nsta][nt][9] array (one strided copy)
+    int rc = synchronize();
+    if (rc) return rc;
+    if (nsta_ <= 0 || it1 <= it0) return CGFDM_OK;
+    if (it0 < 0 || it1 > d_.nt) {
+      set_error("station rows out of range");
+      return CGFDM_ERR_ARG;
+    }
+    const size_t pitch = sizeof(float) * 9 * (size_t)d_.nt;
+    CUDA_TRY(cudaMemcpy2D(wave + (size_t)it0 * 9, pitch, sta_wave_ + (size_t)it0 * 9, pitch,
+                          sizeof(float) * 9 * (size_t)(it1 - it0), nsta_,
+                          cudaMemcpyDeviceToHost));
+    return CGFDM_OK;
+  }
+
   int get_pgv(float *pgv) override {
     int rc = synchronize();
     if (rc) return rc;

@@ -26,6 +26,7 @@ class Engine {
   virtual int synchronize() = 0;
   virtual int steps_done() const = 0;
   virtual int get_stations(float *wave) = 0;
+  virtual int get_station_rows(float *wave, int it0, int it1) = 0;
   virtual int get_pgv(float *pgv) = 0;
   virtual int get_wavefield(float *w) = 0;
   virtual int get_free_surface(float *v3) = 0;

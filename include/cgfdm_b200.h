@@ -200,6 +200,55 @@ int cgfdm_batch_set_graph(cgfdm_batch *b, int32_t on);
 int cgfdm_batch_synchronize(cgfdm_batch *b);
 int cgfdm_batch_destroy(cgfdm_batch *b);
 
+/* ---- serving: a request loop with continuous batching -------------------
+ * No counterpart in the reference.  A server owns one device and a worker
+ * thread.  cgfdm_server_submit queues a simulation (the cgfdm_propagate
+ * inputs, copied) from any thread and returns at once.  The worker admits
+ * queued requests in arrival order while their device footprint
+ * (cgfdm_device_bytes) fits the HBM budget, keeps their wavefields resident,
+ * and advances all admitted requests of one precision together as one batch
+ * (cgfdm_batch) by chunk_steps steps per round -- the batches of different
+ * precisions on their own streams, overlapping on the device.  After each
+ * round the new seismogram rows of every request are copied back
+ * (cgfdm_server_read_rows reads them while the request runs), finished
+ * requests release their memory, and requests that arrived meanwhile join
+ * the next round.  Each request's results equal a lone run bit for bit.
+ * cgfdm_server_stats: [0] p50 and [1] p99 time from submission to the first
+ * streamed seismogram chunk (ms), [2] p50 and [3] p99 time to completion
+ * (ms), [4] aggregate grid-point updates per second (Gpt/s) from the first
+ * submission to the last completion, [5] completed requests, [6] seconds
+ * the worker spent in rounds, [7] peak admitted device bytes. */
+#define CGFDM_REQ_QUEUED 0
+#define CGFDM_REQ_RUNNING 1
+#define CGFDM_REQ_DONE 2
+#define CGFDM_REQ_FAILED 3
+
+typedef struct {
+  int64_t hbm_budget_bytes; /* admission budget; 0 = free device memory minus 4 GiB */
+  int32_t chunk_steps;      /* steps per round (seismograms stream back per round); 0 = 100 */
+  int32_t device;
+  int32_t use_graph;        /* 1: each batch step is replayed as a CUDA graph */
+} cgfdm_server_opts;
+
+typedef struct cgfdm_server cgfdm_server;
+int cgfdm_server_create(const cgfdm_server_opts *opts, cgfdm_server **out);
+int cgfdm_server_submit(cgfdm_server *s, const cgfdm_desc *desc, const float *cjm,
+                        const float *rdz, int32_t point_src, const int32_t *point_xyz,
+                        float rickerfc, const int64_t *src_index, const float *moment_rate,
+                        int64_t npts, int32_t src_nt, float src_dt, const int32_t *sta_xyz,
+                        int32_t nsta, int64_t *id);
+/* state (CGFDM_REQ_*) and the number of steps streamed back so far */
+int cgfdm_server_poll(cgfdm_server *s, int64_t id, int32_t *state, int32_t *steps);
+/* copies rows [from, upto) of every station into wave [nsta][nt][9] */
+int cgfdm_server_read_rows(cgfdm_server *s, int64_t id, int32_t from, float *wave,
+                           int32_t *upto);
+/* blocks until the request ends; copies its seismograms [nsta][nt][9] and PGV
+ * map [ny][nx][2] (either may be NULL) and latencies (ms: to the first
+ * chunk, to completion), then forgets the request */
+int cgfdm_server_wait(cgfdm_server *s, int64_t id, float *wave, float *pgv, double *lat_ms2);
+int cgfdm_server_stats(cgfdm_server *s, double *out8);
+int cgfdm_server_destroy(cgfdm_server *s);
+
 /* ---- one RK stage without any device allocation ------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * while they run -- a serving process that splits all of HBM into fixed pools
