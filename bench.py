@@ -260,6 +260,167 @@ def measure_accuracy(cgfdm, w, prec, kern, device, nsteps, setup):
             "max_abs_ref_v": float(np.abs(sta_ref).max())}
 
 
+# --------------------------------------------------------------------------
+# batched scenarios (c4) and serving (c5)
+# --------------------------------------------------------------------------
+def _setup_scenario(cgfdm, w, prec):
+    d = tempfile.mkdtemp(prefix="cgfdm_bench_")
+    try:
+        write_workload(dict(w, name="s"), d)
+        return cgfdm.setup_from_directory(d, prec)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def _sim_of(cgfdm, setup, prec, nt, device):
+    d0 = setup["desc"]
+    sim = cgfdm.Simulation(cgfdm.make_desc(d0.nx, d0.ny, d0.nz, d0.npml, d0.dh, d0.dt, nt, prec,
+                                           cgfdm.KERNEL_AUTO, device))
+    sim.set_tile_rows(16)
+    sim.set_model(setup["cjm"], setup["rdz"])
+    if setup["point"] is not None:
+        sim.set_point_source(*setup["point"], setup["rickerfc"])
+    if setup["src_index"].size:
+        sim.set_fault_source(setup["src_index"], setup["moment_rate"], setup["src_nt"],
+                             setup["src_dt"], scaled=True)
+    sim.set_stations(setup["stations"])
+    return sim
+
+
+def bench_batch(args, cgfdm, torch, local, prec):
+    """48 seeded scenarios (NX, NY in [121, 401], NZ in [101, 201], own
+    medium, hill and double-couple source) advanced together as one batch
+    (persistent streaming launches spanning all of them, one CUDA graph per
+    step) against the same scenarios run back to back alone."""
+    n = args.batch_n
+    total = args.warmup + args.steps + 2
+    setups = [_setup_scenario(cgfdm, S.sample_scenario(1000 + q, nsteps=total), prec)
+              for q in range(n)]
+    pts = [s["desc"].nx * s["desc"].ny * s["desc"].nz for s in setups]
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    alone_ms = 0.0
+    for st in setups:  # back to back
+        sim = _sim_of(cgfdm, st, prec, total, local)
+        sim.run(args.warmup, stream.cuda_stream)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        sim.run(args.steps, stream.cuda_stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        alone_ms += ev0.elapsed_time(ev1)
+        sim.close()
+    sims = [_sim_of(cgfdm, st, prec, total, local) for st in setups]
+    batch = cgfdm.Batch(sims, graph=True)
+    batch.run(args.warmup, stream.cuda_stream)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        batch.run(args.steps, stream.cuda_stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    batch.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    batch.close()
+    for sim in sims:
+        sim.close()
+    upd = float(sum(pts)) * args.steps
+    return {
+        "metric": "aggregate Gpt-updates/s, batched scenarios", "value": upd / (ms / 1e3) / 1e9,
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": _dtype(args.precision), "data": "synthetic",
+        "config": {"workload": "c4-batched-%d-scenarios" % n, "precision": args.precision,
+                   "points_total": int(sum(pts)), "points_min": int(min(pts)),
+                   "points_max": int(max(pts)), "graph": True, "tile_rows": 16,
+                   "steps_note": "bounded sample of the 1500-step runs"},
+        "serial": {"value": upd / (alone_ms / 1e3) / 1e9, "unit": UNIT,
+                   "note": "the same scenarios run alone back to back (no batch, no graph)"},
+        "speedup_vs_serial": alone_ms / ms,
+        "clocks": clk.summary(),
+    }
+
+
+def bench_serving(args, cgfdm, torch, local):
+    """A seeded Poisson stream of requests (grid points log-uniform in
+    [1e6, 5e7], steps uniform in [500, 3000] times --step-scale, FP32 or
+    FP16 each) through the library's server (continuous batching, graphs,
+    budget 160 GB), against serial single-request FP32 on the same GPU."""
+    rng = np.random.default_rng(7)
+    nreq = args.requests
+    rate = float(rng.uniform(2.0, 20.0))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    reqs = []
+    for q in range(nreq):
+        points = float(np.exp(rng.uniform(math.log(1e6), math.log(5e7))))
+        steps = max(1, int(round(rng.integers(500, 3001) * args.step_scale)))
+        prec = cgfdm.FP16 if rng.random() < 0.5 else cgfdm.FP32
+        w = S.sample_scenario(2000 + q, points=points, nsteps=steps + 2)
+        reqs.append((_setup_scenario(cgfdm, w, prec), prec, steps))
+    log("serving: %d requests generated" % nreq)
+
+    def submit_args(st, prec, steps):
+        d0 = st["desc"]
+        desc = cgfdm.make_desc(d0.nx, d0.ny, d0.nz, d0.npml, d0.dh, d0.dt, steps, prec,
+                               cgfdm.KERNEL_AUTO, local)
+        fault = st["src_index"].size > 0
+        return desc, dict(point=st["point"], rickerfc=st["rickerfc"],
+                          src_index=st["src_index"] if fault else None,
+                          moment_rate=st["moment_rate"] if fault else None,
+                          src_nt=st["src_nt"], src_dt=st["src_dt"], stations=st["stations"])
+
+    chunk = max(1, int(round(100 * args.step_scale)))
+    free = torch.cuda.mem_get_info(local)[0]
+    budget = int(min(160e9, free - 8e9))
+    with cgfdm.Server(hbm_budget_bytes=budget, chunk=chunk, device=local, graph=True) as srv:
+        with ClockSampler(local) as clk:
+            t0 = time.perf_counter()
+            ids = []
+            for q, (st, prec, steps) in enumerate(reqs):
+                delay = arrivals[q] - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                desc, kw = submit_args(st, prec, steps)
+                ids.append(srv.submit(desc, st["cjm"], st["rdz"], **kw))
+            for rid in ids:
+                srv.wait(rid)
+            wall = time.perf_counter() - t0
+        stats = srv.stats()
+    upd = float(sum(st["desc"].nx * st["desc"].ny * st["desc"].nz * steps
+                    for st, _, steps in reqs))
+    # serial single-request FP32: each request alone, end to end (upload, run, results)
+    t_serial = 0.0
+    for st, _, steps in reqs:
+        desc, kw = submit_args(st, cgfdm.FP32, steps)
+        t1 = time.perf_counter()
+        cgfdm.propagate(desc, st["cjm"], st["rdz"], **kw)
+        t_serial += time.perf_counter() - t1
+    return {
+        "metric": "serving: aggregate Gpt-updates/s with p50/p99 latency", "value": stats["gpts"],
+        "unit": UNIT, "n_gpus": 1, "steps": int(sum(s for _, _, s in reqs)), "warmup": 0,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 and f16-storage/f32 (per request)", "data": "synthetic",
+        "config": {"workload": "c5-serving-%d-requests" % nreq, "arrival_rate_per_s": rate,
+                   "step_scale": args.step_scale, "chunk_steps": chunk,
+                   "hbm_budget_bytes": budget, "graph": True,
+                   "fp16_requests": sum(1 for _, p, _ in reqs if p == cgfdm.FP16)},
+        "latency_ms": {"first_seismogram_p50": stats["first_p50_ms"],
+                       "first_seismogram_p99": stats["first_p99_ms"],
+                       "completion_p50": stats["done_p50_ms"],
+                       "completion_p99": stats["done_p99_ms"]},
+        "wall_s": wall, "peak_admitted_bytes": stats["peak_bytes"],
+        "serial_fp32": {"value": upd / t_serial / 1e9, "unit": UNIT, "seconds": t_serial,
+                        "note": "each request alone through cgfdm_propagate, FP32, back to back"},
+        "speedup_vs_serial": stats["gpts"] / (upd / t_serial / 1e9),
+        "clocks": clk.summary(),
+    }
+
+
+def _dtype(p):
+    return {"fp32": "f32", "fp64": "f64", "fp16": "f16-storage/f32", "bf16": "bf16-storage/f32"}[p]
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -281,6 +442,10 @@ def main():
                     help="streaming-kernel tile height (0: the library's autotuner)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-steps", type=int, default=20)
+    ap.add_argument("--batch-n", type=int, default=48, help="scenarios of --workload c4")
+    ap.add_argument("--requests", type=int, default=32, help="requests of --workload c5")
+    ap.add_argument("--step-scale", type=float, default=0.1,
+                    help="--workload c5: request step counts are U[500, 3000] times this")
     ap.add_argument("--accuracy-steps", type=int, default=0,
                     help="also run this many steps in FP64 and in --precision through "
                          "propagate() and report the relative L2 error of the station "
@@ -292,6 +457,10 @@ def main():
 
     if args.impl == "reference":
         if rank != 0:
+            return 0
+        if args.workload in ("c4", "c5"):
+            print(json.dumps({"impl": "reference", "unavailable": "the reference runs one "
+                              "scenario per process: no batched or serving mode"}))
             return 0
         w = make_workload(args.workload, args.warmup + args.steps + 2)
         cores = os.cpu_count() or 1
@@ -328,6 +497,15 @@ def main():
                                 device_id=torch.device("cuda", local))
     prec = {"fp32": cgfdm.FP32, "fp16": cgfdm.FP16, "bf16": cgfdm.BF16, "fp64": cgfdm.FP64}[
         args.precision]
+    if args.workload in ("c4", "c5"):
+        line = (bench_batch(args, cgfdm, torch, local, prec) if args.workload == "c4"
+                else bench_serving(args, cgfdm, torch, local))
+        if rank == 0:
+            print(json.dumps(line))
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
     kern = {"auto": cgfdm.KERNEL_AUTO, "exact": cgfdm.KERNEL_EXACT,
             "stream": cgfdm.KERNEL_STREAM}[args.kernel]
 

@@ -187,3 +187,49 @@ def write_run_dir(dirpath, p, stations=None, terrain=None, layers=None, source=N
 
 def _as_bytes(x):
     return x.tobytes() if isinstance(x, np.ndarray) else bytes(x)
+
+
+def sample_scenario(seed, nx_range=(121, 401), nz_range=(101, 201), points=None,
+                    nsteps=100, dt=0.008, npml=12):
+    """One seeded scenario of the batched-serving workloads: grid sizes
+    uniform in the ranges (or, with ``points`` given, NX = NY chosen so that
+    NX * NY * NZ is close to it), a Gaussian hill of amplitude U[0, 2000] m,
+    a three-layer medium with seeded layer depths and velocities (+-5 %), a
+    double-couple point source of random strike / dip / rake at 1-10 km depth
+    with a Ricker source time function of f0 U[0.5, 3] Hz, and a 5 x 5
+    station lattice on the surface.  Returns dict(params, terrain, layers,
+    source, stations)."""
+    rng = np.random.default_rng(seed)
+    nz = int(rng.integers(nz_range[0], nz_range[1] + 1))
+    if points is None:
+        nx = int(rng.integers(nx_range[0], nx_range[1] + 1))
+        ny = int(rng.integers(nx_range[0], nx_range[1] + 1))
+    else:
+        nx = ny = max(40, int(round(math.sqrt(points / nz))))
+    dh = 100.0
+    depth_km = (nz - 1) * dh / 1000.0
+    p = params(NX=nx, NY=ny, NZ=nz, DH=dh, DT=dt, TMAX=(nsteps + 0.5) * dt,
+               **{"Depth(km)": depth_km}, centerX=0, centerY=0, nPML=npml, useTerrain=1,
+               useMedium=1, LayeredModel=1, useMultiSource=1,
+               **{"useSingleSource(ricker)": 0}, IT_SKIP=10 ** 7, out="out")
+    amp = float(rng.uniform(0.0, 2000.0))
+    terrain = gaussian_hill(p, amp=amp, x0=nx * dh / 2, y0=ny * dh / 2,
+                            width=max(nx, ny) * dh / 8)
+    j = lambda: float(rng.uniform(0.95, 1.05))
+    d1, d2 = float(rng.uniform(1.5, 2.5)), float(rng.uniform(6.0, 10.0))
+    layers = layered_bytes([(d1, 2.6 * j(), 4.5 * j(), 2.3), (d2, 3.35 * j(), 5.8 * j(), 2.6),
+                            (1000.0, 3.75 * j(), 6.5 * j(), 2.8)])
+    f0 = float(rng.uniform(0.5, 3.0))
+    zdepth = float(rng.uniform(1000.0, min(10000.0, 0.6 * depth_km * 1000.0)))
+    x = float(rng.uniform(0.3, 0.7)) * nx * dh
+    y = float(rng.uniform(0.3, 0.7)) * ny * dh
+    nt_src = nsteps + 8
+    src = double_couple_point(x, y, -zdepth, m0=1e16, mu=3.2e10,
+                              strike=float(rng.uniform(0, 360)), dip=float(rng.uniform(10, 90)),
+                              rake=float(rng.uniform(-180, 180)), nt=nt_src, dt=dt,
+                              stf=lambda t: ricker_rate(t, f0, 1.2 / f0))
+    stations = {"S%02d" % (a * 5 + b): [int(nx * (a + 1) / 6), int(ny * (b + 1) / 6), nz - 1]
+                for a in range(5) for b in range(5)}
+    return {"params": p, "terrain": terrain, "layers": layers, "source": src,
+            "stations": stations}
+
