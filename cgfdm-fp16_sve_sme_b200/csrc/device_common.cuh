@@ -73,12 +73,17 @@ template <typename S, typename R> __device__ __forceinline__ R rnd(R v) {
 }
 
 // One PML slab on the device: slab-local box, offset into the padded grid,
-// the derivative axis, and its four auxiliary buffers ([npos][9] values of
-// type A, AoS as pml_deriv.cpp:199-207; float except in the FP64 run).
+// the derivative axis, and its four auxiliary buffers of type A (float except
+// in the FP64 run).  On the device the 9 auxiliary fields of a slab are
+// stored field-major, [9][np] (value v of slab point pos at v * np + pos,
+// pos x-fastest), so that a warp's consecutive points read and write
+// consecutive addresses; the host interface keeps the reference's [pos][9]
+// (pml_deriv.cpp:199-207) and converts.
 template <typename A> struct SlabDev {
   int n0, n1, n2;        // extent along x, y, z
   int off0, off1, off2;  // padded index of the slab origin
   int axis;              // 0 = x, 1 = y, 2 = z
+  long long np;          // n0 * n1 * n2
   const A *ain;          // stage-input auxiliaries
   A *aout;               // stage-output auxiliaries
   const A *am;           // step-start auxiliaries

@@ -480,16 +480,18 @@ template <typename S> class EngineT : public Engine {
     if (W) CUDA_TRY(upload_repacked(W, bufs[in_of[irk]], 9));
     if (t) CUDA_TRY(upload_repacked(t, T_, 9));
     if (aux && aux_total_ > 0) {
-      // host layout: per slab {Aux, t, m}
+      // host layout: per slab {Aux, t, m}, each [pos][9]; device: [9][pos]
       std::vector<R> a(aux_total_), tt(aux_total_), mm(aux_total_);
       long long off = 0, dst = 0;
       for (int s = 0; s < 5; ++s) {
-        long long n = g_.slab_pts[s] * 9;
-        for (long long q = 0; q < n; ++q) {
-          a[dst + q] = aux[off + q];
-          tt[dst + q] = aux[off + n + q];
-          mm[dst + q] = aux[off + 2 * n + q];
-        }
+        const long long np = g_.slab_pts[s], n = np * 9;
+        for (long long p = 0; p < np; ++p)
+          for (int v = 0; v < 9; ++v) {
+            const long long hq = p * 9 + v, dq = dst + v * np + p;
+            a[dq] = aux[off + hq];
+            tt[dq] = aux[off + n + hq];
+            mm[dq] = aux[off + 2 * n + hq];
+          }
         off += 3 * n;
         dst += n;
       }
@@ -513,12 +515,14 @@ template <typename S> class EngineT : public Engine {
       CUDA_TRY(cudaMemcpy(mm.data(), auxbuf(0), sizeof(R) * aux_total_, cudaMemcpyDeviceToHost));
       long long off = 0, src = 0;
       for (int s = 0; s < 5; ++s) {
-        long long n = g_.slab_pts[s] * 9;
-        for (long long q = 0; q < n; ++q) {
-          aux[off + q] = (float)o[src + q];
-          aux[off + n + q] = (float)tt[src + q];
-          aux[off + 2 * n + q] = (float)mm[src + q];
-        }
+        const long long np = g_.slab_pts[s], n = np * 9;
+        for (long long p = 0; p < np; ++p)
+          for (int v = 0; v < 9; ++v) {
+            const long long hq = p * 9 + v, dq = src + v * np + p;
+            aux[off + hq] = (float)o[dq];
+            aux[off + n + hq] = (float)tt[dq];
+            aux[off + 2 * n + hq] = (float)mm[dq];
+          }
         off += 3 * n;
         src += n;
       }
@@ -626,6 +630,7 @@ template <typename S> class EngineT : public Engine {
       SlabDev<R> &sl = a.slab[s];
       sl.n0 = g_.slab_n[s][0]; sl.n1 = g_.slab_n[s][1]; sl.n2 = g_.slab_n[s][2];
       sl.off0 = g_.slab_off[s][0]; sl.off1 = g_.slab_off[s][1]; sl.off2 = g_.slab_off[s][2];
+      sl.np = g_.slab_pts[s];
       sl.axis = s % 3;
       sl.ain = auxbuf(in_of[irk]) + off;
       sl.aout = auxbuf(out_of[irk]) + off;

@@ -94,8 +94,8 @@ int stage_noalloc(const cgfdm_stage_buffers &b, cudaStream_t st, unsigned char *
   a.DT = b.dt;
   a.fb1 = b.fb1; a.fb2 = b.fb2; a.fb3 = b.fb3;
   a.irk = b.irk;
-  // PML slabs x1 y1 z1 x2 y2 (no top z slab), each [pos][9] with pos
-  // x-fastest inside the slab, concatenated in that order (pml_deriv.cpp:14-31)
+  // PML slabs x1 y1 z1 x2 y2 (no top z slab), each field-major [9][pos] with
+  // pos x-fastest inside the slab, concatenated in that order
   a.nslab = b.npml > 0 ? 5 : 0;
   long long off = 0;
   for (int s = 0; s < a.nslab; ++s) {
@@ -106,6 +106,7 @@ int stage_noalloc(const cgfdm_stage_buffers &b, cudaStream_t st, unsigned char *
     SlabDev<float> &sl = a.slab[s];
     sl.n0 = n[0]; sl.n1 = n[1]; sl.n2 = n[2];
     sl.off0 = o[0]; sl.off1 = o[1]; sl.off2 = o[2];
+    sl.np = (long long)n[0] * n[1] * n[2];
     sl.axis = ax;
     sl.ain = b.aux_in + off;
     sl.aout = b.aux_out + off;

@@ -191,7 +191,8 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
     const R alpha = prof[l], bt = prof[nax + l], dl = prof[2 * nax + l];
     const R ad = dl + alpha;
     const long long pos = i0 + (long long)j0 * sl.n0 + (long long)k0 * sl.n0 * sl.n1;
-    const R *ain = sl.ain + pos * 9;
+    const long long np = sl.np;
+    const R *ain = sl.ain + pos;  // value v at ain[v * np]
     R m[3], dv[3], dt[6], term[9], ha[9];
     metric(cjm, num, c, ax, m);
 #pragma unroll
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
     elastic(m, dv, dt, mu, lam, b * (R)CRHO_OF<S>::v, term);
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
-      const R av = ain[v];
+      const R av = ain[v * np];
       ha[v] = (term[v] - ad * av) * DT;
       h[v] = rnd<S>(h[v] + -bt * av * DT);
     }
@@ -221,28 +222,29 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
       for (int v = 3; v < 9; ++v) ha[v] = ha[v] + t[v] * DT;
     }
     // pml_rk.cpp:15-69
-    R *aout = sl.aout + pos * 9;
-    R *at = sl.at + pos * 9;
-    const R *am = sl.am + pos * 9;
+    R *aout = sl.aout + pos;
+    R *at = sl.at + pos;
+    const R *am = sl.am + pos;
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
       const R hv = ha[v];
+      const long long q = v * np;
       switch (a.irk) {
         case 0: {
-          const R mv = ain[v];
-          at[v] = mv + (R)kB1 * hv;
-          aout[v] = mv + (R)kA2rk * hv;
+          const R mv = ain[q];
+          at[q] = mv + (R)kB1 * hv;
+          aout[q] = mv + (R)kA2rk * hv;
         } break;
         case 1:
-          at[v] = at[v] + (R)kB2 * hv;
-          aout[v] = am[v] + (R)kA3rk * hv;
+          at[q] = at[q] + (R)kB2 * hv;
+          aout[q] = am[q] + (R)kA3rk * hv;
           break;
         case 2:
-          at[v] = at[v] + (R)kB3 * hv;
-          aout[v] = am[v] + hv;
+          at[q] = at[q] + (R)kB3 * hv;
+          aout[q] = am[q] + hv;
           break;
         default:
-          aout[v] = at[v] + (R)kB4 * hv;
+          aout[q] = at[q] + (R)kB4 * hv;
       }
     }
   }

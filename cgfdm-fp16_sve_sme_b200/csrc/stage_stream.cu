@@ -68,12 +68,8 @@ template <typename S, int TYv> struct Geo {
   static constexpr int OFF_C = NW * W_BYTES;
   static constexpr int OFF_M = OFF_C + NC * C_BYTES;
   static constexpr int OFF_BAR = OFF_M + NM * M_BYTES;
-  // PML variant: one 32 x 9 float staging buffer per warp
-  static constexpr int OFF_P = (OFF_BAR + 8 * (NW + NC + NM) + 127) / 128 * 128;
-  static constexpr int P_BYTES = (NTHR / 32) * 32 * 9 * 4;
   static constexpr int SMEM = OFF_BAR + 8 * (NW + NC + NM) + 128;
-  static constexpr int SMEM_P = OFF_P + P_BYTES + 128;
-  static_assert(SMEM_P <= 232448, "shared memory budget");
+  static_assert(SMEM <= 232448, "shared memory budget");
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -135,110 +131,57 @@ __device__ __forceinline__ long long slab_pos(const SlabDev<float> &sl, int i, i
   return (i - sl.off0) + (long long)(j - sl.off1) * sl.n0 + (long long)(k - sl.off2) * sl.n0 * sl.n1;
 }
 
-// PML of one derivative direction for the lanes of a warp that lie in slab
-// `sid` (pml_deriv.cpp:199-237 and pml_rk.cpp:15-69).  Those lanes are
-// consecutive in x, so their auxiliary records ([pos][9], pos x-fastest)
-// form one contiguous run: the warp reads and writes the run flat (lane l
-// takes elements l, l + 32, ...), fully coalesced, with each owner's elastic
-// combination E staged through the warp's buffer `buf` (32 x 9 floats).  The
-// -beta * Aux * DT term comes back through the same buffer into h.
-// prof: alpha, beta, d of the axis (nax each); the profile index is
-// lbase + lstep * (point within the run).
-// L2 prefetch (a hint) of the 16-byte-aligned part of n floats at p; the run
-// is rounded inward, so nothing outside it is touched.
-__device__ __forceinline__ void prefetch_run(const float *p, int n) {
-  const unsigned long long b = ((unsigned long long)p + 15) & ~15ull;
-  const unsigned long long e = (unsigned long long)(p + n) & ~15ull;
-  if (e > b)
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b), "r"((unsigned)(e - b))
-                 : "memory");
-}
-
-__device__ __forceinline__ void pml_warp(unsigned vm, const SlabDev<float> &sl, bool mine,
-                                         long long pos, const float E[9], float h[9], float *buf,
-                                         const float *prof, int nax, int lidx, int lstep,
-                                         int irk, float DT, long long next) {
-  // next: offset in records of the same run one output plane further in the
-  // sweep (0: the item has no further plane); it is prefetched into L2
-  // vm: the lanes of this warp that take part (the valid points of the row)
-  const unsigned lane = threadIdx.x & 31;
-  const unsigned m = __ballot_sync(vm, mine);
-  if (!m) return;
-  const int l0 = __ffs(m) - 1, nact = __popc(m);
-  const long long pos0 = __shfl_sync(vm, pos, l0);
-  const int lbase = __shfl_sync(vm, lidx, l0);
-  if (mine) {
+// PML auxiliary update of one slab point (pml_deriv.cpp:199-237,
+// pml_rk.cpp:15-69) given the direction's elastic combination E; adds
+// -beta * Aux * DT into h.  The auxiliaries are field-major on the device
+// (value v at v * np + pos), so the lanes of a warp, consecutive points of
+// the slab, touch consecutive addresses.  Fields go three at a time, each
+// group's loads issued before its stores (the buffers do not overlap).
+__device__ __forceinline__ void pml_point(const SlabDev<float> &sl, long long pos, const float E[9],
+                                          float dl, float ad, float bt, float DT, int irk,
+                                          float h[9]) {
+  const long long np = sl.np;
+  const float *__restrict__ ain = sl.ain + pos;
+  const float *__restrict__ am = sl.am + pos;
+  float *__restrict__ aout = sl.aout + pos;
+  float *__restrict__ at = sl.at + pos;
+  // three fields at a time: their auxiliary input, what the stage adds the
+  // increment to (m in stages 1-2, t in stage 3) and t itself (stages 1-2)
 #pragma unroll
-    for (int v = 0; v < 9; ++v) buf[(lane - l0) * 9 + v] = E[v];
-  }
-  __syncwarp(vm);
-  const int n = nact * 9;
-  const float *__restrict__ ain = sl.ain + pos0 * 9;
-  const float *__restrict__ am = sl.am + pos0 * 9;
-  float *__restrict__ aout = sl.aout + pos0 * 9;
-  float *__restrict__ at = sl.at + pos0 * 9;
-  // the participating lanes (nv of them, this one of rank r) cover the run
-  // flat: element f = f0 + r + nv * q, 9 per lane per batch (one batch when
-  // the whole warp takes part)
-  const int nv = __popc(vm), r = __popc(vm & ((1u << lane) - 1u));
-  if (next && r == 0) {
-    const long long pn = (pos0 + next) * 9;
-    prefetch_run(sl.ain + pn, n);
-    if (irk == 1 || irk == 2) prefetch_run(sl.am + pn, n);
-    if (irk >= 1) prefetch_run(sl.at + pn, n);
-  }
-  for (int f0 = 0; f0 < n; f0 += 9 * nv) {
-    // every load of the batch first: the auxiliary input, and what the stage
-    // adds its increment to (m in stages 1-2, t in stage 3) plus t (stages 1-2)
-    float av[9], bv[9], tv[9];
+  for (int g = 0; g < 9; g += 3) {
+    float av[3], bv[3], tv[3];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      const int f = f0 + r + nv * q;
-      av[q] = bv[q] = tv[q] = 0.0f;
-      if (f < n) {
-        av[q] = ain[f];
-        if (irk == 1 || irk == 2) {
-          bv[q] = am[f];
-          tv[q] = at[f];
-        } else if (irk == 3) {
-          bv[q] = at[f];
-        }
-      }
+    for (int u = 0; u < 3; ++u) {
+      const long long q = (g + u) * np;
+      av[u] = ain[q];
+      bv[u] = irk == 0 ? 0.0f : irk == 3 ? at[q] : am[q];
+      tv[u] = (irk == 1 || irk == 2) ? at[q] : 0.0f;
     }
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      const int f = f0 + r + nv * q;
-      if (f < n) {
-        const int l = lbase + lstep * (f / 9);
-        const float dl = prof[2 * nax + l], bt = prof[nax + l], ad = prof[l] + dl;
-        const float a = av[q];
-        const float ha = (dl * buf[f] - ad * a) * DT;
-        buf[f] = -bt * a * DT;
-        switch (irk) {
-          case 0:
-            at[f] = a + kB1 * ha;
-            aout[f] = a + kA2rk * ha;
-            break;
-          case 1:
-            at[f] = tv[q] + kB2 * ha;
-            aout[f] = bv[q] + kA3rk * ha;
-            break;
-          case 2:
-            at[f] = tv[q] + kB3 * ha;
-            aout[f] = bv[q] + ha;
-            break;
-          default:
-            aout[f] = bv[q] + kB4 * ha;
-        }
+    for (int u = 0; u < 3; ++u) {
+      const int v = g + u;
+      const long long q = v * np;
+      const float a = av[u];
+      const float ha = (dl * E[v] - ad * a) * DT;
+      h[v] -= bt * a * DT;
+      switch (irk) {
+        case 0:
+          at[q] = a + kB1 * ha;
+          aout[q] = a + kA2rk * ha;
+          break;
+        case 1:
+          at[q] = tv[u] + kB2 * ha;
+          aout[q] = bv[u] + kA3rk * ha;
+          break;
+        case 2:
+          at[q] = tv[u] + kB3 * ha;
+          aout[q] = bv[u] + ha;
+          break;
+        default:
+          aout[q] = bv[u] + kB4 * ha;
       }
     }
   }
-  __syncwarp(vm);
-  if (mine) {
-#pragma unroll
-    for (int v = 0; v < 9; ++v) h[v] += buf[(lane - l0) * 9 + v];
-  }
-  __syncwarp(vm);
 }
 
 struct Maps {
@@ -453,16 +396,13 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
     // per-column PML beta times DT
     const int ic = valid ? i : HALO, jc = valid ? j : HALO;
     const float bxd = px[L.nx_ + ic] * DT, byd = py[L.ny_ + jc] * DT;
-    // PML variant: the x (x1/x2) and y (y1/y2) slab of this column, and the
-    // valid lanes of this warp row (member mask of the warp-wide PML steps)
+    // PML variant: the x (x1/x2) and y (y1/y2) slab of this column
     int sx = -1, sy = -1;
     if (PMLK && valid && a.nslab) {
       const int np = a.npml;
       sx = i < HALO + np ? 0 : i >= L.nx_ - HALO - np ? 3 : -1;
       sy = j < HALO + np ? 1 : j >= L.ny_ - HALO - np ? 4 : -1;
     }
-    const unsigned vmask = PMLK ? __ballot_sync(0xffffffffu, valid) : 0u;
-    float *pbuf = PMLK ? (float *)(smem + G::OFF_P) + (tid / 32) * 32 * 9 : nullptr;
 
     // z window in registers: physical slot n mod 5 holds input plane q_n; the
     // plane loop is unrolled five times so that every slot index is a
@@ -506,7 +446,6 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         const float mu = ldv(cf + 9 * NTHR + cidx), lam = ldv(cf + 10 * NTHR + cidx);
         const float bu = ldv(cf + 11 * NTHR + cidx) * (float)CRHO_OF<S>::v;
         const float bzd = pz[L.nz_ + k] * DT;
-        const bool more = o + 1 < nout;  // this item has a further output plane
         float h[9], Lr[9], E[9];
         // x direction
 #pragma unroll
@@ -518,11 +457,9 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         elastic9(mx, Lr, mu, lam, bu, E);
 #pragma unroll
         for (int v = 0; v < 9; ++v) h[v] = bxd * E[v];
-        if (PMLK && a.nslab) {
-          pml_warp(vmask, a.slab[0], sx == 0, slab_pos(a.slab[0], i, j, k), E, h, pbuf, px,
-                   L.nx_, i, 1, irk, DT, more ? DIR * (long long)a.slab[0].n0 * a.slab[0].n1 : 0);
-          pml_warp(vmask, a.slab[3], sx == 3, slab_pos(a.slab[3], i, j, k), E, h, pbuf, px,
-                   L.nx_, i, 1, irk, DT, more ? DIR * (long long)a.slab[3].n0 * a.slab[3].n1 : 0);
+        if (PMLK && sx >= 0) {  // profile values d, alpha + d, beta at this x
+          const float dl = px[2 * L.nx_ + i], bt = px[L.nx_ + i], ad = px[i] + dl;
+          pml_point(a.slab[sx], slab_pos(a.slab[sx], i, j, k), E, dl, ad, bt, DT, irk, h);
         }
         // y direction
 #pragma unroll
@@ -534,11 +471,9 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         elastic9(my, Lr, mu, lam, bu, E);
 #pragma unroll
         for (int v = 0; v < 9; ++v) h[v] += byd * E[v];
-        if (PMLK && a.nslab) {
-          pml_warp(vmask, a.slab[1], sy == 1, slab_pos(a.slab[1], i, j, k), E, h, pbuf, py,
-                   L.ny_, j, 0, irk, DT, more ? DIR * (long long)a.slab[1].n0 * a.slab[1].n1 : 0);
-          pml_warp(vmask, a.slab[4], sy == 4, slab_pos(a.slab[4], i, j, k), E, h, pbuf, py,
-                   L.ny_, j, 0, irk, DT, more ? DIR * (long long)a.slab[4].n0 * a.slab[4].n1 : 0);
+        if (PMLK && sy >= 0) {
+          const float dl = py[2 * L.ny_ + j], bt = py[L.ny_ + j], ad = py[j] + dl;
+          pml_point(a.slab[sy], slab_pos(a.slab[sy], i, j, k), E, dl, ad, bt, DT, irk, h);
         }
         // z direction: W[k - m*DIR] for m = -1..3 sits in slots P0 (q = k + DIR) .. P4
 #pragma unroll
@@ -548,9 +483,10 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         elastic9(mz, Lr, mu, lam, bu, E);
 #pragma unroll
         for (int v = 0; v < 9; ++v) h[v] += bzd * E[v];
-        if (PMLK && a.nslab && k < HALO + a.npml)
-          pml_warp(vmask, a.slab[2], true, slab_pos(a.slab[2], i, j, k), E, h, pbuf, pz, L.nz_,
-                   k, 0, irk, DT, more ? DIR * (long long)a.slab[2].n0 * a.slab[2].n1 : 0);
+        if (PMLK && a.nslab && k < HALO + a.npml) {
+          const float dlz = pz[2 * L.nz_ + k], btz = pz[L.nz_ + k], adz = pz[k] + dlz;
+          pml_point(a.slab[2], slab_pos(a.slab[2], i, j, k), E, dlz, adz, btz, DT, irk, h);
+        }
         // RK4 combination (wave_rk.cpp:13-99)
         const S *ms = (const S *)(smem + G::OFF_M + ((fm0 + o) % NM) * G::M_BYTES);
         const S *ts = ms + 9 * NTHR;
@@ -588,7 +524,8 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
     };
     int n = 0;
     if (PMLK) {
-      // one loop body (small code): the window moves down one slot per plane
+      // one loop body (the PML variant's code is large; unrolled it no longer
+      // fits the instruction cache): the window moves down one slot per plane
 #pragma unroll 1
       for (; n < nplanes; ++n) {
         if (!iter(std::integral_constant<int, 0>{}, n)) break;
@@ -652,7 +589,7 @@ cudaError_t launch_variant(const StageArgs<S> &a, const Maps &maps, const Work &
   using G = Geo<S, TYv>;
   static int attr_dev = -1;
   auto kern = stage_stream_kernel<S, TYv, FB1, FB2, FB3, PMLK>;
-  const int smem = PMLK ? G::SMEM_P : G::SMEM;
+  const int smem = G::SMEM;
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
@@ -751,7 +688,7 @@ cudaError_t launch_batch_variant(const BatchParams<S> &p, int items, int *err, i
   static_assert(sizeof(BatchParams<S>) <= 32000, "kernel parameter space");
   static int attr_dev = -1;
   auto kern = stage_stream_batch_kernel<S, FB1, FB2, FB3, PMLK>;
-  const int smem = PMLK ? G::SMEM_P : G::SMEM;
+  const int smem = G::SMEM;
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {

@@ -268,8 +268,10 @@ int cgfdm_server_destroy(cgfdm_server *s);
  * plane = px * _ny_, fs = roundup(plane * _nz_, 32); field f of padded point
  * (i, j, k) at element f * fs + xoff + i + j * px + k * plane.  rdz is
  * 2 x (_nx_*_ny_) x 9 float.  The four auxiliary buffers are float, each the
- * slabs x1 y1 z1 x2 y2 concatenated ([pos][9], pos x-fastest), as many floats
- * as cgfdm_aux_floats reports for a handle of the same grid.  Stage irk reads
+ * slabs x1 y1 z1 x2 y2 concatenated, every slab field-major [9][np] (value v
+ * of slab point pos at v * np + pos, pos x-fastest, np the slab's points;
+ * the reference's own order is [pos][9]), as many floats as cgfdm_aux_floats
+ * reports for a handle of the same grid.  Stage irk reads
  * w_in, cjm, rdz, w_m (stages 1-2), t (stages 1-3), aux_in, aux_m (stages
  * 1-2), aux_t (stages 1-3), and writes w_out, t (stages 0-2), aux_out and
  * aux_t (stages 0-2).

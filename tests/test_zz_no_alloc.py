@@ -93,15 +93,26 @@ def test_noalloc_stage_matches_handle_stage(gpu_available, precision, case):
     def from_hbm(buf, nf):
         return view(buf, nf).float().cpu().numpy().reshape(-1)
 
-    # per slab {Aux, t, m} -> the concatenations cgfdm_stage_buffers takes
-    sizes = [9 * n for n in scenarios.slab_points(p)]
+    # per slab {Aux, t, m} in the reference's [pos][9] -> the concatenations
+    # cgfdm_stage_buffers takes: every slab field-major, [9][pos]
+    npts = list(scenarios.slab_points(p))
+    sizes = [9 * n for n in npts]
     parts = {"a": [], "t": [], "m": []}
     off = 0
-    for n9 in sizes:
+    for n in npts:
         for k, key in enumerate("atm"):
-            parts[key].append(st["aux"][off + k * n9: off + (k + 1) * n9])
-        off += 3 * n9
-    aux = {k: torch.from_numpy(np.concatenate(v)).to(dev) for k, v in parts.items()}
+            aos = st["aux"][off + k * 9 * n: off + (k + 1) * 9 * n]
+            parts[key].append(aos.reshape(n, 9).T.reshape(-1))
+        off += 27 * n
+    aux = {k: torch.from_numpy(np.ascontiguousarray(np.concatenate(v))).to(dev)
+           for k, v in parts.items()}
+
+    def to_aos(soa):  # device order back to the reference's, slab by slab
+        out, o = [], 0
+        for n in npts:
+            out.append(soa[o:o + 9 * n].reshape(9, n).T.reshape(-1))
+            o += 9 * n
+        return np.concatenate(out)
 
     w_in = to_hbm(st["W"], 9)
     w_m = w_in if irk == 0 else to_hbm(st["m"], 9)  # stage 0 reads its input as m
@@ -137,8 +148,8 @@ def test_noalloc_stage_matches_handle_stage(gpu_available, precision, case):
         if call == 1:  # (the first call of a process may load the library's module)
             assert free_after == free_before, (free_before, free_after)
         got = {"W": (from_hbm(w_out, 9), ref["W"]), "t": (from_hbm(t, 9), ref["t"]),
-               "aux_out": (aux_out.cpu().numpy(), ref_out),
-               "aux_t": (aux_t.cpu().numpy(), ref_t)}
+               "aux_out": (to_aos(aux_out.cpu().numpy()), ref_out),
+               "aux_t": (to_aos(aux_t.cpu().numpy()), ref_t)}
         for key, (a, r) in got.items():
             err = rel_l2(a, r)
             assert err <= TOL, (call, key, err)
