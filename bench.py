@@ -421,6 +421,18 @@ def _dtype(p):
     return {"fp32": "f32", "fp64": "f64", "fp16": "f16-storage/f32", "bf16": "bf16-storage/f32"}[p]
 
 
+def replica_throughput(torch, dist, seconds, points, steps, world, device):
+    """Whole-job throughput of N independent replicas (one per rank, the
+    same work each): the slowest rank's time bounds the job, so the value is
+    world * points * steps / max over ranks of the time.  Returns (Gpt/s,
+    max seconds).  Every rank must call it (one all-reduce)."""
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+    if dist is not None and world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    tmax = float(t.item())
+    return world * float(points) * steps / tmax / 1e9, tmax
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -560,11 +572,8 @@ def main():
     ks = sim.kernel_stats()
     stage_ms, stage_n = float(tm[1]), int(tm[2])
     sim.close()
-    ms_t = torch.tensor([ms], device="cuda")
-    if dist:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = ws * npts * args.steps / (ms_max / 1e3) / 1e9
+    value, ms_max = replica_throughput(torch, dist, ms / 1e3, npts, args.steps, ws, "cuda")
+    ms_max *= 1e3
 
     # end to end through the drop-in with host buffers (propagate())
     e2e_steps = args.e2e_steps
@@ -578,10 +587,7 @@ def main():
         moment_rate=setup["moment_rate"] if setup["src_index"].size else None,
         src_nt=setup["src_nt"], src_dt=setup["src_dt"], stations=sta)
     e2e_s = time.perf_counter() - t0
-    e2e_t = torch.tensor([e2e_s], device="cuda")
-    if dist:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = ws * npts * e2e_steps / float(e2e_t.item()) / 1e9
+    e2e_value, e2e_max = replica_throughput(torch, dist, e2e_s, npts, e2e_steps, ws, "cuda")
     h2d = cjm.nbytes + setup["rdz"].nbytes + setup["moment_rate"].nbytes + \
         setup["src_index"].nbytes + sta.nbytes
     d2h = out_sta.nbytes + out_pgv.nbytes + out_fs.nbytes
@@ -669,7 +675,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
                     "d2h_bytes_per_step": d2h / e2e_steps, "steps": e2e_steps,
-                    "seconds": float(e2e_t.item())},
+                    "seconds": e2e_max},
             "gpu_launches": ks["launches"],
             "clocks": clk.summary(),
         }
