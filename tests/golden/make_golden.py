@@ -13,6 +13,10 @@ stage_small.npz
     profiles -- and, for four (irk, FB) cases, one RK stage of the reference's
     hot path applied to the same seeded input state (wavefield, RK buffers and
     PML auxiliaries).
+run_point_fp16.npz
+    The point-source run through the reference's scalar FP16 build (outputs
+    only; the inputs are those of run_point.npz).  The FP16 build overflows
+    on the finite-fault run (non-finite seismograms), so it has no fixture.
 run_point.npz, run_fault.npz
     Complete reference runs (main.cpp -> run.cpp -> propagate.cpp) of small
     configurations: a flat half-space with the smoothed explosive point
@@ -117,6 +121,24 @@ def run_fixture(name, sc, dumper):
         shutil.rmtree(work)
 
 
+def run_fixture_fp16(name, sc):
+    """The reference's scalar FP16 build (FLOAT = _Float16, Cv/Cs/Crho
+    scaling) on the same inputs as an FP32 run fixture: its outputs only."""
+    exe = os.path.join(REF_DIR, "cgfdm_ref_fp16")
+    work = tempfile.mkdtemp(prefix="cgfdm_golden_")
+    try:
+        scenarios.write_inputs(sc, work)
+        subprocess.check_call([exe], cwd=work, stdout=subprocess.DEVNULL)
+        res = scenarios.read_outputs(sc, os.path.join(work, sc["params"]["out"]))
+        out = {"params_json": np.array(json.dumps(sc["params"])),
+               "stations_json": np.array(json.dumps(sc["stations"]))}
+        for k, v in res.items():
+            out["out_" + k] = v
+        np.savez_compressed(os.path.join(HERE, name), **out)
+    finally:
+        shutil.rmtree(work)
+
+
 def main():
     if not os.path.isdir(REF_SRC):
         sys.exit("reference sources not found at %s" % REF_SRC)
@@ -126,6 +148,8 @@ def main():
     stage_fixture(exe)
     run_fixture("run_point.npz", scenarios.run_point(), exe)
     run_fixture("run_fault.npz", scenarios.run_fault(), exe)
+    # (the FP16 build overflows on run_fault: its seismograms are not finite)
+    run_fixture_fp16("run_point_fp16.npz", scenarios.run_point())
     print("golden fixtures written to", HERE)
 
 
