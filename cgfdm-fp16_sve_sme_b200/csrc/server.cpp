@@ -1,20 +1,21 @@
 // Request loop with continuous batching (cgfdm_server_* of the C ABI).
 //
 // Requests (one simulation each: grid, model, sources, stations, precision)
-// are queued by submit() from any host thread.  One worker thread owns the
-// GPU work:
-//   * admission: queued requests are admitted in arrival order while their
-//     device footprint (engine_device_bytes) fits the HBM budget; a request
-//     larger than the whole budget fails at submission;
-//   * rounds: all admitted requests of one precision advance together as one
-//     batch (batched persistent streaming launches, optionally one CUDA graph
-//     per step) by `chunk` steps, or fewer when a member has fewer left; the
-//     FP32, FP16, BF16 and FP64 batches of a round run on their own streams,
-//     so their work overlaps on the device;
-//   * after a round, each member's new seismogram rows are copied into the
-//     request's host buffer (streamed back chunk by chunk), finished requests
-//     copy their PGV map, release their device memory and leave the batch,
-//     and requests that arrived meanwhile are admitted for the next round.
+// are queued by submit() from any host thread.  Two threads do the work:
+//   * admission thread: queued requests are admitted in arrival order while
+//     their device footprint (engine_device_bytes) fits the HBM budget; it
+//     creates each engine and uploads the inputs on the engine's own stream,
+//     overlapping the rounds that are running; a request larger than the
+//     whole budget fails at submission;
+//   * worker thread, in rounds: all running requests of one precision
+//     advance together as one batch (batched persistent streaming launches,
+//     optionally one CUDA graph per step) by `chunk` steps, or fewer when a
+//     member has fewer left; the FP32, FP16, BF16 and FP64 batches of a round
+//     run on their own streams, so their work overlaps on the device; after a
+//     round each member's new seismogram rows are copied into the request's
+//     host buffer (streamed back chunk by chunk), finished requests copy
+//     their PGV map, release their device memory and leave the batch, and the
+//     requests admitted meanwhile join the next round.
 // Wavefields stay resident on the device from admission to completion.
 // Latencies are measured from submission: to the first streamed seismogram
 // chunk, and to completion.
@@ -107,6 +108,7 @@ class Server {
         return CGFDM_ERR_CUDA;
       }
     worker_ = std::thread([this] { loop(); });
+    admitter_ = std::thread([this] { admit_loop(); });
     return CGFDM_OK;
   }
 
@@ -117,6 +119,8 @@ class Server {
       stopping_ = true;
     }
     cv_.notify_all();
+    work_cv_.notify_all();
+    if (admitter_.joinable()) admitter_.join();
     if (worker_.joinable()) worker_.join();
     cudaSetDevice(opts_.device);
     batches_.clear();
@@ -254,36 +258,51 @@ class Server {
     r.admitted = false;
   }
 
+  // Admission thread: creates the engines of queued requests and uploads
+  // their inputs (on each engine's own stream) while the worker's rounds run.
+  void admit_loop() {
+    cudaSetDevice(opts_.device);
+    for (;;) {
+      Request *r = nullptr;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] {
+          return stopping_ ||
+                 (!queue_.empty() && used_ + reqs_[queue_.front()]->bytes <= budget_);
+        });
+        if (stopping_) return;
+        r = reqs_[queue_.front()].get();
+        used_ += r->bytes;  // reserved before the engine exists
+        r->admitted = true;
+        peak_bytes_ = std::max(peak_bytes_, used_);
+        queue_.pop_front();
+      }
+      int rc = admit(*r);
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (rc) {
+          fail(*r, rc);
+        } else {
+          r->state = CGFDM_REQ_RUNNING;
+          ready_.push_back(r);
+        }
+      }
+      done_cv_.notify_all();
+      work_cv_.notify_all();
+    }
+  }
+
   void loop() {
     cudaSetDevice(opts_.device);
     std::vector<Request *> active;
     for (;;) {
-      // admission (arrival order, by free HBM)
-      std::vector<Request *> admit_now;
       {
         std::unique_lock<std::mutex> lk(mu_);
-        cv_.wait(lk, [&] { return stopping_ || !queue_.empty() || !active.empty(); });
+        work_cv_.wait(lk, [&] { return stopping_ || !ready_.empty() || !active.empty(); });
         if (stopping_) return;
-        while (!queue_.empty()) {
-          Request *r = reqs_[queue_.front()].get();
-          if (used_ + r->bytes > budget_) break;
-          used_ += r->bytes;
-          r->admitted = true;
-          peak_bytes_ = std::max(peak_bytes_, used_);
-          queue_.pop_front();
-          admit_now.push_back(r);
-        }
-      }
-      for (Request *r : admit_now) {
-        int rc = admit(*r);
-        std::lock_guard<std::mutex> lk(mu_);
-        if (rc) {
-          fail(*r, rc);
-          done_cv_.notify_all();
-        } else {
-          r->state = CGFDM_REQ_RUNNING;
-          active.push_back(r);
-        }
+        // requests admitted since the last round join this one
+        active.insert(active.end(), ready_.begin(), ready_.end());
+        ready_.clear();
       }
       if (active.empty()) continue;
       const auto t0 = Clock::now();
@@ -309,6 +328,7 @@ class Server {
             fail(*r, rc);
           }
           done_cv_.notify_all();
+          cv_.notify_all();
           continue;
         }
         ran.push_back({m, k});
@@ -361,6 +381,7 @@ class Server {
         busy_s_ += std::chrono::duration<double>(Clock::now() - t0).count();
       }
       done_cv_.notify_all();
+      if (!retire.empty()) cv_.notify_all();  // memory came free
     }
   }
 
@@ -383,12 +404,13 @@ class Server {
   cgfdm_server_opts opts_;
   int64_t budget_ = 0, used_ = 0, peak_bytes_ = 0;
   std::mutex mu_;
-  std::condition_variable cv_, done_cv_;
+  std::condition_variable cv_, done_cv_, work_cv_;  // admission, results, rounds
+  std::vector<Request *> ready_;  // admitted, not yet in a round
   std::deque<int64_t> queue_;
   std::map<int64_t, std::unique_ptr<Request>> reqs_;
   int64_t next_id_ = 0;
   bool stopping_ = false;
-  std::thread worker_;
+  std::thread worker_, admitter_;
   cudaStream_t streams_[4] = {};
   std::map<int, std::pair<std::vector<Engine *>, std::unique_ptr<BatchBase>>> batches_;
   std::vector<double> lat_first_, lat_done_;
