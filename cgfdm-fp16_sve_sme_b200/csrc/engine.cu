@@ -132,9 +132,13 @@ template <typename S> class EngineT : public Engine {
     CUDA_TRY(cudaMalloc(&step_, sizeof(int)));
     CUDA_TRY(cudaMemsetAsync(step_, 0, sizeof(int), own_stream_));
     for (int q = 0; q < 2; ++q) CUDA_TRY(cudaEventCreate(&ev_[q]));
+    // opposite PML slabs that overlap (nPML above half the grid, a point in
+    // both x1 and x2) are left to the exact-order kernel, which applies every
+    // slab of a point; the streaming kernel applies one slab per axis
+    const bool overlap = g_.npml > 0 && (2 * g_.npml > g_.nx || 2 * g_.npml > g_.ny);
     use_stream_ = stage_stream_supported<S>() && d_.kernel != CGFDM_KERNEL_EXACT &&
-                  g_.nz > 3;
-    if (d_.kernel == CGFDM_KERNEL_STREAM && !stage_stream_supported<S>()) {
+                  g_.nz > 3 && !overlap;
+    if (d_.kernel == CGFDM_KERNEL_STREAM && !stage_stream_supported<S>() ) {
       set_error("the streaming kernel does not support this precision");
       return CGFDM_ERR_ARG;
     }

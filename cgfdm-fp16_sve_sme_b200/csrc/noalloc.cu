@@ -123,7 +123,10 @@ int stage_noalloc(const cgfdm_stage_buffers &b, cudaStream_t st, unsigned char *
   int rc = encode_stream_maps<S>(a.win, a.cjm, a.wm, a.t, L, maps);
   if (rc) return rc;
   int *err = (int *)scratch, *counter = (int *)(scratch + 4);
-  const int ksurf = L.nz_ - HALO - 3;
+  // as a handle does: the exact-order kernel alone when opposite PML slabs
+  // overlap (nPML above half the grid)
+  const bool overlap = b.npml > 0 && (2 * b.npml > b.nx || 2 * b.npml > b.ny);
+  const int ksurf = overlap ? HALO : L.nz_ - HALO - 3;
   StageArgs<S> lower = a;
   lower.kbeg = HALO;
   lower.kend = ksurf;

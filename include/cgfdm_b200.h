@@ -62,7 +62,9 @@ extern "C" {
 #define CGFDM_KERNEL_AUTO 0      /* fastest kernel for the precision */
 #define CGFDM_KERNEL_EXACT 1     /* reference operation order, no FMA contraction:
                                     bit-identical to the reference's FP32 CPU path */
-#define CGFDM_KERNEL_STREAM 2    /* TMA-staged z-streaming fused stage kernel */
+#define CGFDM_KERNEL_STREAM 2    /* TMA-staged z-streaming fused stage kernel (grids
+                                    whose opposite PML slabs overlap, nPML above half
+                                    of nx or ny, run the exact-order kernel) */
 
 typedef struct {
   int32_t nx, ny, nz;     /* interior points (params NX, NY, NZ) */

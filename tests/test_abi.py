@@ -15,7 +15,8 @@ HEADER = os.path.join(ROOT, "include", "cgfdm_b200.h")
 
 
 def declared_functions():
-    text = open(HEADER).read()
+    with open(HEADER) as f:
+        text = f.read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"^\s*[A-Za-z_][\w\s\*]*?\b(cgfdm_\w+)\s*\(", text, flags=re.M)))
 

@@ -39,7 +39,7 @@ def _rank(rank, world, port, out):
 
 def test_replica_throughput_two_ranks():
     world = 2
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()  # no fork of this process
     mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
     for rank in range(world):
         value, tmax = out[rank]
