@@ -12,10 +12,11 @@ LIB_PATH = os.path.join(PKG_ROOT, "lib", "libcgfdm_b200.so")
 
 OK = 0
 ERR = {1: "ARG", 100: "PARAMS", 110: "CFL", 130: "PML", 180: "NO_SOURCE", 181: "SOURCE",
-       200: "IO", 300: "CUDA", 301: "NOMEM", 302: "NO_KERNEL", 303: "TIMEOUT", 304: "STATE"}
+       200: "IO", 300: "CUDA", 301: "NOMEM", 302: "NO_KERNEL", 303: "TIMEOUT", 304: "STATE",
+       305: "CANCELLED"}
 FP32, FP16, BF16, FP64 = 0, 1, 2, 3
 KERNEL_AUTO, KERNEL_EXACT, KERNEL_STREAM = 0, 1, 2
-REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = 0, 1, 2, 3, 4
 
 
 class CgfdmError(RuntimeError):
@@ -88,6 +89,7 @@ SIGNATURES = {
     "cgfdm_get_kernel_stats": (C.c_int, [P, P]),
     "cgfdm_set_tile_rows": (C.c_int, [P, I32]),
     "cgfdm_set_graph": (C.c_int, [P, I32]),
+    "cgfdm_inject_fault": (C.c_int, [P, I32]),
     "cgfdm_batch_create": (C.c_int, [P, I32, C.POINTER(P)]),
     "cgfdm_batch_run": (C.c_int, [P, I32, P]),
     "cgfdm_batch_set_graph": (C.c_int, [P, I32]),
@@ -100,6 +102,7 @@ SIGNATURES = {
     "cgfdm_server_read_rows": (C.c_int, [P, I64, I32, P, C.POINTER(I32)]),
     "cgfdm_server_wait": (C.c_int, [P, I64, P, P, P]),
     "cgfdm_server_stats": (C.c_int, [P, P]),
+    "cgfdm_server_cancel": (C.c_int, [P, I64]),
     "cgfdm_server_destroy": (C.c_int, [P]),
     "cgfdm_propagate": (C.c_int, [C.POINTER(Desc), P, P, I32, P, F, P, P, I64, I32, F, P, I32,
                                   P, P, P]),

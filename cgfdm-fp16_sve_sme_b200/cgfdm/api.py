@@ -108,6 +108,11 @@ class Simulation:
         check(lib().cgfdm_get_timing(self._h, _ptr(ms)))
         return ms
 
+    def inject_fault(self, kind=1):
+        """Failure-detection tests: the next streaming launch leaves one load
+        unissued so that a bounded device wait expires (CGFDM_ERR_TIMEOUT)."""
+        check(lib().cgfdm_inject_fault(self._h, int(kind)))
+
     def set_graph(self, on=True):
         """Replay each step of run() as a CUDA graph (results are identical)."""
         check(lib().cgfdm_set_graph(self._h, int(on)))
@@ -248,12 +253,15 @@ class Server:
         return upto.value
 
     def wait(self, rid):
-        nsta, nt, ny, nx = self._shape.pop(rid)
+        nsta, nt, ny, nx = self._shape.pop(rid, (0, 0, 0, 0))
         wave = np.zeros((nsta, nt, 9), np.float32)
         pgv = np.zeros((ny, nx, 2), np.float32)
         lat = np.zeros(2, np.float64)
         check(lib().cgfdm_server_wait(self._s, rid, _ptr(wave), _ptr(pgv), _ptr(lat)))
         return wave, pgv, (float(lat[0]), float(lat[1]))
+
+    def cancel(self, rid):
+        check(lib().cgfdm_server_cancel(self._s, rid))
 
     def stats(self):
         v = np.zeros(8, np.float64)

@@ -186,6 +186,11 @@ int cgfdm_get_timing(cgfdm_handle *h, float *ms3) {
   return h->eng->get_timing(ms3);
 }
 
+int cgfdm_inject_fault(cgfdm_handle *h, int32_t kind) {
+  H_OR_FAIL(h);
+  return h->eng->inject_fault(kind);
+}
+
 int cgfdm_set_graph(cgfdm_handle *h, int32_t on) {
   H_OR_FAIL(h);
   return h->eng->set_graph(on != 0);

@@ -106,6 +106,10 @@ template <typename S> struct StageArgs {
   int npml;
   float rDH, DT;
   int fb1, fb2, fb3, irk;
+  // failure-detection tests only: the streaming kernel leaves one input-plane
+  // load of its first work item unissued, so that the bounded wait on it
+  // expires (no memory is touched); 0 in every normal launch
+  int drop_one_load;
 };
 
 }  // namespace cgfdm

@@ -405,9 +405,21 @@ template <typename S> class EngineT : public Engine {
     int flag = 0;
     CUDA_TRY(cudaMemcpy(&flag, err_flag_, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag) {
+      // reported once; the stage outputs of the failed launch are not valid
+      CUDA_TRY(cudaMemset(err_flag_, 0, sizeof(int)));
       set_error("a bounded device-side wait of the streaming kernel expired");
       return CGFDM_ERR_TIMEOUT;
     }
+    return CGFDM_OK;
+  }
+
+  int inject_fault(int kind) override {
+    if (kind != 0 && kind != 1) {
+      set_error("unknown fault kind");
+      return CGFDM_ERR_ARG;
+    }
+    drop_next_load_ = kind == 1;
+    drop_graphs();
     return CGFDM_OK;
   }
 
@@ -717,6 +729,8 @@ template <typename S> class EngineT : public Engine {
       StageArgs<S> b = a;
       b.kbeg = HALO;
       b.kend = ksurf;
+      b.drop_one_load = drop_next_load_ ? 1 : 0;
+      drop_next_load_ = false;
       CUDA_TRY(launch_stage_stream<S>(b, tmap_[in_of[irk]], err_flag_, err_flag_ + 1, st,
                                       ev ? ev[1] : nullptr, &launches_,
                                       tile_rows_ ? tile_rows_ : 16));
@@ -845,6 +859,7 @@ template <typename S> class EngineT : public Engine {
   int stage_used_ = 0;
   int launches_ = 0;          // kernels launched by the last run()
   int tile_rows_ = 0;         // streaming-kernel tile height; 0 = autotune at the first run()
+  bool drop_next_load_ = false;  // fault injection for failure-detection tests
   int *step_ = nullptr;       // device copy of it_
   float *moment_tab_ = nullptr;            // point-source moment per step
   int *fit_tab_ = nullptr;                 // fault interpolation index per step (-1: ended)

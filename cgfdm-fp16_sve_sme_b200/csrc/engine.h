@@ -40,6 +40,7 @@ class Engine {
   virtual int get_kernel_stats(double *out8) = 0;
   virtual int set_tile_rows(int rows) = 0;
   virtual int set_graph(bool on) = 0;
+  virtual int inject_fault(int kind) = 0;
   virtual const cgfdm_desc &desc() const = 0;
 };
 

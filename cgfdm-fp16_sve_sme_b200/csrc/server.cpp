@@ -54,6 +54,7 @@ struct Request {
   float src_dt = 0;
   int64_t bytes = 0;
   bool admitted = false;  // its bytes count against the budget
+  bool cancel = false;    // cancellation asked while admitted: retire after the round
   // results
   std::vector<float> wave, pgv;
   int steps = 0;          // steps whose seismograms are in `wave`
@@ -189,6 +190,30 @@ class Server {
     return CGFDM_OK;
   }
 
+  int cancel(int64_t id) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto f = reqs_.find(id);
+    if (f == reqs_.end()) {
+      set_error("server: unknown request");
+      return CGFDM_ERR_ARG;
+    }
+    Request &r = *f->second;
+    if (r.state == CGFDM_REQ_QUEUED && !r.admitted) {
+      queue_.erase(std::remove(queue_.begin(), queue_.end(), id), queue_.end());
+      r.state = CGFDM_REQ_CANCELLED;
+      r.t_done = Clock::now();
+      done_cv_.notify_all();
+      cv_.notify_all();
+      return CGFDM_OK;
+    }
+    if (r.state == CGFDM_REQ_QUEUED || r.state == CGFDM_REQ_RUNNING) {
+      r.cancel = true;  // the worker retires it after its current round
+      return CGFDM_OK;
+    }
+    set_error("server: the request has already ended");
+    return CGFDM_ERR_STATE;
+  }
+
   int wait(int64_t id, float *wave, float *pgv, double *lat_ms) {
     std::unique_lock<std::mutex> lk(mu_);
     auto f = reqs_.find(id);
@@ -197,7 +222,15 @@ class Server {
       return CGFDM_ERR_ARG;
     }
     Request *r = f->second.get();
-    done_cv_.wait(lk, [&] { return r->state == CGFDM_REQ_DONE || r->state == CGFDM_REQ_FAILED; });
+    done_cv_.wait(lk, [&] {
+      return r->state == CGFDM_REQ_DONE || r->state == CGFDM_REQ_FAILED ||
+             r->state == CGFDM_REQ_CANCELLED;
+    });
+    if (r->state == CGFDM_REQ_CANCELLED) {
+      set_error("server: the request was cancelled");
+      reqs_.erase(f);
+      return CGFDM_ERR_CANCELLED;
+    }
     if (r->state == CGFDM_REQ_FAILED) {
       set_error(r->error_text);
       const int e = r->error;
@@ -357,7 +390,7 @@ class Server {
             }
             r->steps = it1;
           }
-          if (rc || finished) retire.push_back({r, rc});
+          if (rc || finished || r->cancel) retire.push_back({r, rc});
         }
       }
       for (const Retire &x : retire) batches_.erase(x.r->desc.precision);
@@ -373,6 +406,11 @@ class Server {
           }
           used_ -= r->bytes;
           r->admitted = false;
+          if (r->cancel && r->steps < r->desc.nt) {
+            r->state = CGFDM_REQ_CANCELLED;
+            r->t_done = Clock::now();
+            continue;
+          }
           r->t_done = Clock::now();
           t_last_done_ = r->t_done;
           lat_done_.push_back(ms_between(r->t_submit, r->t_done));
@@ -426,6 +464,11 @@ struct cgfdm_server {
 };
 
 extern "C" {
+
+int cgfdm_server_cancel(cgfdm_server *sv, int64_t id) {
+  if (!sv || !sv->s) return CGFDM_ERR_ARG;
+  return sv->s->cancel(id);
+}
 
 int cgfdm_server_create(const cgfdm_server_opts *opts, cgfdm_server **out) {
   if (!opts || !out) return CGFDM_ERR_ARG;

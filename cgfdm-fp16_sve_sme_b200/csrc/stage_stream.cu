@@ -363,6 +363,7 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
     const int xs = c + G::HB, ys = r + (FB2 > 0 ? 1 : 3);
 
     auto issue_w = [&](int n) {
+      if (a.drop_one_load && local == 0 && n == NW - 1) return;  // test hook, see StageArgs
       const unsigned f = fw0 + n, s = f % NW;
       const uint32_t bar = smem_u32(&bw[s]);
       mbar_expect_tx(bar, 9 * BY * BX * G::ES);

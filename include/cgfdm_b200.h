@@ -51,6 +51,7 @@ extern "C" {
 #define CGFDM_ERR_NO_KERNEL 302    /* CUDA extension unusable (no device / wrong arch) */
 #define CGFDM_ERR_TIMEOUT 303      /* a bounded device-side wait expired */
 #define CGFDM_ERR_STATE 304        /* call not valid in the handle's current state */
+#define CGFDM_ERR_CANCELLED 305    /* the server request was cancelled */
 
 /* ---- storage precision of wavefield and coefficients ---- */
 #define CGFDM_FP32 0   /* float everywhere: the reference's FP32 build */
@@ -173,6 +174,17 @@ int cgfdm_get_kernel_stats(cgfdm_handle *h, double *out8);
  * choice is cached per (precision, grid) for the process. */
 int cgfdm_set_tile_rows(cgfdm_handle *h, int32_t rows);
 
+/* Failure-detection testing (no counterpart in the reference): kind 1 makes
+ * the next streaming-kernel launch of the handle leave one tile-plane load
+ * unissued, so that one CTA's bounded wait expires (about 2^31 clock cycles,
+ * a second); the CTA waits for its other copies, sets the error flag and
+ * returns, and the next synchronizing call reports CGFDM_ERR_TIMEOUT once.
+ * No memory is touched and the context stays usable; that stage's outputs
+ * are not valid.  kind 0 clears a pending injection. */
+#define CGFDM_FAULT_NONE 0
+#define CGFDM_FAULT_DROP_LOAD 1
+int cgfdm_inject_fault(cgfdm_handle *h, int32_t kind);
+
 /* Replays each time step of cgfdm_run as a CUDA graph (on = 1) instead of
  * launching its kernels one by one; one graph per phase of the step counter
  * mod 8 (the MacCormack signs repeat with period 8), captured on the second
@@ -224,6 +236,7 @@ int cgfdm_batch_destroy(cgfdm_batch *b);
 #define CGFDM_REQ_RUNNING 1
 #define CGFDM_REQ_DONE 2
 #define CGFDM_REQ_FAILED 3
+#define CGFDM_REQ_CANCELLED 4
 
 typedef struct {
   int64_t hbm_budget_bytes; /* admission budget; 0 = free device memory minus 4 GiB */
@@ -248,6 +261,10 @@ int cgfdm_server_read_rows(cgfdm_server *s, int64_t id, int32_t from, float *wav
  * map [ny][nx][2] (either may be NULL) and latencies (ms: to the first
  * chunk, to completion), then forgets the request */
 int cgfdm_server_wait(cgfdm_server *s, int64_t id, float *wave, float *pgv, double *lat_ms2);
+/* cancels a request: a queued one leaves the queue at once; an admitted one
+ * stops after the round it is in, and its device memory is released; wait()
+ * then returns CGFDM_ERR_CANCELLED */
+int cgfdm_server_cancel(cgfdm_server *s, int64_t id);
 int cgfdm_server_stats(cgfdm_server *s, double *out8);
 int cgfdm_server_destroy(cgfdm_server *s);
 

@@ -104,3 +104,32 @@ def test_server_rejects_request_above_budget(gpu_available):
         with pytest.raises(cgfdm.CgfdmError) as e:
             srv.submit(d, sc["cjm"], sc["rdz"], **kw)
         assert e.value.code == 301
+
+
+@pytest.mark.gpu
+def test_server_cancel_queued_and_running(gpu_available):
+    """Cancelling a queued request and a running one: both end as cancelled
+    (their memory released), the others still equal their lone runs."""
+    mix = _mix()[:4]
+    budget = max(cgfdm.device_bytes(_request(sc, p)[0]) for sc, p in mix)  # one at a time
+    with cgfdm.Server(hbm_budget_bytes=budget, chunk=3, graph=True) as srv:
+        ids = []
+        for q, (sc, prec) in enumerate(mix):
+            d, kw = _request(sc, prec)
+            if q == 0:
+                d.nt = 3000  # long enough to be cancelled while it runs
+            ids.append(srv.submit(d, sc["cjm"], sc["rdz"], **kw))
+        srv.cancel(ids[3])  # still queued behind the others
+        deadline = time.time() + 60
+        while srv.poll(ids[0])[1] == 0 and time.time() < deadline:
+            time.sleep(0.005)
+        srv.cancel(ids[0])  # running (some rows streamed back already)
+        for q in (0, 3):
+            with pytest.raises(cgfdm.CgfdmError) as e:
+                srv.wait(ids[q])
+            assert e.value.code == 305
+        for q in (1, 2):
+            wave, pgv, _ = srv.wait(ids[q])
+            ref_w, ref_p = _alone(*mix[q])
+            np.testing.assert_array_equal(wave, ref_w)
+        assert srv.stats()["completed"] == 2
