@@ -13,6 +13,9 @@ stage_small.npz
     profiles -- and, for four (irk, FB) cases, one RK stage of the reference's
     hot path applied to the same seeded input state (wavefield, RK buffers and
     PML auxiliaries).
+c1_halfspace.npz
+    The homogeneous half-space benchmark configuration (161 x 161 x 101,
+    1000 steps, double-couple point source, 25 stations), one rank.
 run_point_fp16.npz
     The point-source run through the reference's scalar FP16 build (outputs
     only; the inputs are those of run_point.npz).  The FP16 build overflows
@@ -139,6 +142,28 @@ def run_fixture_fp16(name, sc):
         shutil.rmtree(work)
 
 
+def c1_fixture():
+    """The half-space benchmark configuration (scenarios.c1, 1000 steps)
+    through the reference's FP32 build on one rank: seismograms, PGV and the
+    free-surface snapshots (inputs are regenerated from scenarios.c1; the
+    setup products are left out, the host setup is tested bit for bit
+    elsewhere)."""
+    sc = scenarios.c1()
+    exe = os.path.join(REF_DIR, "cgfdm_ref_fp32")
+    work = tempfile.mkdtemp(prefix="cgfdm_golden_")
+    try:
+        scenarios.write_inputs(sc, work)
+        subprocess.check_call([exe], cwd=work, stdout=subprocess.DEVNULL)
+        res = scenarios.read_outputs(sc, os.path.join(work, sc["params"]["out"]))
+        out = {"params_json": np.array(json.dumps(sc["params"])),
+               "stations_json": np.array(json.dumps(sc["stations"]))}
+        for k, v in res.items():
+            out["out_" + k] = v
+        np.savez_compressed(os.path.join(HERE, "c1_halfspace.npz"), **out)
+    finally:
+        shutil.rmtree(work)
+
+
 def main():
     if not os.path.isdir(REF_SRC):
         sys.exit("reference sources not found at %s" % REF_SRC)
@@ -148,6 +173,7 @@ def main():
     stage_fixture(exe)
     run_fixture("run_point.npz", scenarios.run_point(), exe)
     run_fixture("run_fault.npz", scenarios.run_fault(), exe)
+    c1_fixture()
     # (the FP16 build overflows on run_fault: its seismograms are not finite)
     run_fixture_fp16("run_point_fp16.npz", scenarios.run_point())
     print("golden fixtures written to", HERE)

@@ -80,6 +80,34 @@ def write_inputs(sc, dirpath):
                     source=sc.get("source"))
 
 
+def c1():
+    """The homogeneous half-space benchmark configuration: 161 x 161 x 101
+    at DH = 100 m (Vp 6000, Vs 3464, rho 2670, the reference's homogeneous
+    medium), DT = 0.008 s, 1000 steps, 12-cell PML; one double-couple point
+    source (strike 0, dip 90, rake 0, M0 = 1e16) at x = y = 8 km, 2 km deep,
+    through the multi-source path, with the moment-rate time function of the
+    reference's single source (singleSource.cpp:47-53: the derivative of a
+    Ricker wavelet, f0 = 1.5 Hz) centred at t0 = 1.0 s; 25 surface stations
+    on a 5 x 5 lattice, 3 km apart; the free-surface snapshot at the last
+    step."""
+    nt = 1000
+    dt = 0.008
+    p = S.params(NX=161, NY=161, NZ=101, DH=100.0, DT=dt, TMAX=8.0001, nPML=12,
+                 centerX=0, centerY=0, useMultiSource=1, **{"useSingleSource(ricker)": 0},
+                 IT_SKIP=999, sliceFreeSurf=1, out="out")
+    f0, t0 = 1.5, 1.0
+
+    def stf(t):
+        r = np.pi * f0 * (t - t0)
+        return np.pi * f0 * 2.0 * r * (2.0 * r * r - 3.0) * np.exp(-r * r)
+
+    src = S.double_couple_point(8000.0, 8000.0, -2000.0, m0=1e16, mu=2670.0 * 3464.0 ** 2,
+                                strike=0.0, dip=90.0, rake=0.0, nt=nt + 2, dt=dt, stf=stf)
+    stations = {"S%d%d" % (a, b): [20 + 30 * a, 20 + 30 * b, 100]
+                for a in range(5) for b in range(5)}
+    return {"params": p, "stations": stations, "source": src}
+
+
 def read_outputs(sc, outdir):
     """Reads the reference's single-rank outputs (station.cpp:382-405,
     PGV.cpp:103-111, data_io.cpp:323-495)."""
