@@ -314,6 +314,101 @@ int cgfdm_free_setup(cgfdm_setup *s) {
   return CGFDM_OK;
 }
 
+namespace {
+
+// Slice and free-surface snapshots of run_directory, written without
+// stalling the time loop (data_io.cpp:323-495 file layout): each snapshot is
+// packed on the work stream into a device staging slot, copied into a
+// pinned host slot on a copy stream, and written to its files only when the
+// slot comes round again (three slots), so the GPU keeps stepping meanwhile.
+class SnapshotPipe {
+ public:
+  struct File {
+    std::string name;
+    char axis;
+    size_t off, n;
+  };
+  ~SnapshotPipe() {
+    for (auto &s : slots_) {
+      if (s.dev) cudaFree(s.dev);
+      if (s.host) cudaFreeHost(s.host);
+      if (s.packed) cudaEventDestroy(s.packed);
+      if (s.copied) cudaEventDestroy(s.copied);
+    }
+    if (copy_) cudaStreamDestroy(copy_);
+  }
+  int init(size_t floats) {
+    floats_ = floats;
+    if (cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking) != cudaSuccess) return fail();
+    for (auto &s : slots_) {
+      if (cudaMalloc(&s.dev, sizeof(float) * floats) != cudaSuccess ||
+          cudaMallocHost(&s.host, sizeof(float) * floats) != cudaSuccess ||
+          cudaEventCreateWithFlags(&s.packed, cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventCreateWithFlags(&s.copied, cudaEventDisableTiming) != cudaSuccess)
+        return fail();
+    }
+    return CGFDM_OK;
+  }
+  // The next slot's device buffer (after writing out what it held).
+  int begin(float **dev) {
+    Slot &s = slots_[next_];
+    int rc = drain(s);
+    if (rc) return rc;
+    *dev = s.dev;
+    return CGFDM_OK;
+  }
+  // The slot begun last is packed (on `work`): copy it out, remember files.
+  int commit(cudaStream_t work, std::vector<File> files) {
+    Slot &s = slots_[next_];
+    if (cudaEventRecord(s.packed, work) != cudaSuccess ||
+        cudaStreamWaitEvent(copy_, s.packed, 0) != cudaSuccess ||
+        cudaMemcpyAsync(s.host, s.dev, sizeof(float) * floats_, cudaMemcpyDeviceToHost, copy_) !=
+            cudaSuccess ||
+        cudaEventRecord(s.copied, copy_) != cudaSuccess)
+      return fail();
+    s.files = std::move(files);
+    s.pending = true;
+    next_ = (next_ + 1) % kSlots;
+    return CGFDM_OK;
+  }
+  int finish() {
+    for (int q = 0; q < kSlots; ++q) {
+      int rc = drain(slots_[(next_ + q) % kSlots]);
+      if (rc) return rc;
+    }
+    return CGFDM_OK;
+  }
+
+ private:
+  static constexpr int kSlots = 3;
+  struct Slot {
+    float *dev = nullptr, *host = nullptr;
+    cudaEvent_t packed = nullptr, copied = nullptr;
+    std::vector<File> files;
+    bool pending = false;
+  };
+  int drain(Slot &s) {
+    if (!s.pending) return CGFDM_OK;
+    if (cudaEventSynchronize(s.copied) != cudaSuccess) return fail();
+    s.pending = false;
+    for (const File &f : s.files) {
+      int rc = cgfdm::write_slice_file(f.name, f.axis, s.host + f.off, f.n);
+      if (rc) return rc;
+    }
+    return CGFDM_OK;
+  }
+  int fail() {
+    set_error(std::string("snapshot pipeline: ") + cudaGetErrorString(cudaGetLastError()));
+    return CGFDM_ERR_CUDA;
+  }
+  Slot slots_[kSlots];
+  size_t floats_ = 0;
+  int next_ = 0;
+  cudaStream_t copy_ = nullptr;
+};
+
+}  // namespace
+
 int cgfdm_run_directory(const char *run_dir, int32_t precision, int32_t kernel, int32_t device) {
   if (!run_dir) return CGFDM_ERR_ARG;
   return guarded([&] {
@@ -343,34 +438,49 @@ int cgfdm_run_directory(const char *run_dir, int32_t precision, int32_t kernel, 
     const double cv_inv = (precision == CGFDM_FP16 || precision == CGFDM_BF16) ? 1.0 / 5.0e3 : 1.0;
     const int at[3] = {s.p.sliceX + 3, s.p.sliceY + 3, s.p.sliceZ + 3};
     const int lim[3] = {s.nx_ - 3, s.ny_ - 3, s.nz_ - 3};
-    std::vector<float> buf;
+    // what one snapshot holds: V slices through sliceX/Y/Z, free-surface V
+    std::vector<std::pair<int, size_t>> slice_axes;  // (axis, points)
+    size_t floats = 0;
+    for (int ax = 0; ax < 3; ++ax) {
+      if (at[ax] < 3 || at[ax] >= lim[ax]) continue;
+      const size_t n = ax == 0 ? (size_t)s.p.NY * s.p.NZ : ax == 1 ? (size_t)s.p.NX * s.p.NZ
+                                                                    : (size_t)s.p.NX * s.p.NY;
+      slice_axes.push_back({ax, n});
+      floats += 3 * n;
+    }
+    const size_t nsurf = (size_t)s.p.NX * s.p.NY;
+    if (s.p.sliceFreeSurf) floats += 3 * nsurf;
+    SnapshotPipe pipe;
+    if (floats > 0 && (rc = pipe.init(floats))) return rc;
+    const char *vn[3] = {"Vx", "Vy", "Vz"};
     for (int it = 0; it < NT; ++it) {
       if ((rc = eng->run(1, nullptr))) return rc;
-      if (it % skip == 0) {
-        char name[512];
-        const char *vn[3] = {"Vx", "Vy", "Vz"};
-        for (int ax = 0; ax < 3; ++ax) {
-          if (at[ax] < 3 || at[ax] >= lim[ax]) continue;
-          size_t n = ax == 0 ? (size_t)s.p.NY * s.p.NZ : ax == 1 ? (size_t)s.p.NX * s.p.NZ
-                                                                  : (size_t)s.p.NX * s.p.NY;
-          buf.resize(n);
-          for (int v = 0; v < 3; ++v) {
-            if ((rc = eng->get_slice(v, ax, at[ax], cv_inv, buf.data()))) return rc;
-            std::snprintf(name, sizeof name, "%s/%s_%d", out.c_str(), vn[v], it);
-            if ((rc = cgfdm::write_slice_file(name, "XYZ"[ax], buf.data(), n))) return rc;
-          }
-        }
-        if (s.p.sliceFreeSurf) {
-          size_t n = (size_t)s.p.NX * s.p.NY;
-          buf.resize(3 * n);
-          if ((rc = eng->get_free_surface(buf.data()))) return rc;
-          for (int v = 0; v < 3; ++v) {
-            std::snprintf(name, sizeof name, "%s/FreeSurf%s_%d", out.c_str(), vn[v], it);
-            if ((rc = cgfdm::write_slice_file(name, 'Z', buf.data() + v * n, n))) return rc;
-          }
+      if (floats == 0 || it % skip != 0) continue;
+      float *dev = nullptr;
+      if ((rc = pipe.begin(&dev))) return rc;
+      std::vector<SnapshotPipe::File> files;
+      size_t off = 0;
+      char name[512];
+      for (const auto &sa : slice_axes) {
+        const int ax = sa.first;
+        for (int v = 0; v < 3; ++v) {
+          if ((rc = eng->enqueue_slice(v, ax, at[ax], cv_inv, dev + off))) return rc;
+          std::snprintf(name, sizeof name, "%s/%s_%d", out.c_str(), vn[v], it);
+          files.push_back({name, "XYZ"[ax], off, sa.second});
+          off += sa.second;
         }
       }
+      if (s.p.sliceFreeSurf) {
+        for (int v = 0; v < 3; ++v) {  // the top interior layer (data_io.cpp:481-491)
+          if ((rc = eng->enqueue_slice(v, 2, s.nz_ - 3 - 1, cv_inv, dev + off))) return rc;
+          std::snprintf(name, sizeof name, "%s/FreeSurf%s_%d", out.c_str(), vn[v], it);
+          files.push_back({name, 'Z', off, nsurf});
+          off += nsurf;
+        }
+      }
+      if ((rc = pipe.commit(eng->work_stream(), std::move(files)))) return rc;
     }
+    if (floats > 0 && (rc = pipe.finish())) return rc;
     if ((rc = eng->synchronize())) return rc;
     if (nsta > 0) {
       std::vector<float> wave((size_t)nsta * NT * 9);

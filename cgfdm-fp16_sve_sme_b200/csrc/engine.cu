@@ -469,6 +469,14 @@ template <typename S> class EngineT : public Engine {
     return CGFDM_OK;
   }
 
+  int enqueue_slice(int field, int axis, int at, double scale, float *dev_out) override {
+    CUDA_TRY(launch_slice_pack<S>(A_ + field * g_.L.fs, g_.L, axis, at, scale, dev_out,
+                                  work_stream()));
+    return CGFDM_OK;
+  }
+
+  cudaStream_t work_stream() const override { return last_stream_ ? last_stream_ : own_stream_; }
+
   int get_slice(int field, int axis, int at, double scale, float *out) override {
     int rc = synchronize();
     if (rc) return rc;

@@ -1,5 +1,7 @@
 // Device-side simulation state of one handle and its time loop.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <memory>
 #include <string>
@@ -31,6 +33,10 @@ class Engine {
   virtual int get_wavefield(float *w) = 0;
   virtual int get_free_surface(float *v3) = 0;
   virtual int get_slice(int field, int axis, int at, double scale, float *out) = 0;
+  // Packs an interior slice of field `field` of the step state (times scale)
+  // into device memory on the stream of the handle's work, without waiting.
+  virtual int enqueue_slice(int field, int axis, int at, double scale, float *dev_out) = 0;
+  virtual cudaStream_t work_stream() const = 0;
   virtual int set_state(int irk, const float *W, const float *t, const float *m,
                         const float *aux) = 0;
   virtual int get_state(float *W, float *t, float *m, float *aux) = 0;

@@ -1,0 +1,56 @@
+"""The half-space benchmark configuration end to end (161 x 161 x 101, 1000
+RK4 steps, 12-cell PML, double-couple point source through the multi-source
+path, 25 surface stations): the reference program on one GPU
+(cgfdm_run_directory) against the reference's own FP32 CPU build
+(tests/golden/c1_halfspace.npz).  The exact-order kernel reproduces every
+seismogram sample, the PGV map and the free-surface snapshots bit for bit;
+the streaming kernel stays within relative L2 1e-5."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import scenarios
+
+pytestmark = pytest.mark.gpu
+cgfdm = pytest.importorskip("cgfdm")
+
+FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c1_halfspace.npz")
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def c1_ref(gpu_available):
+    if not os.path.exists(FIXTURE):
+        pytest.skip("c1 fixture not generated")
+    return np.load(FIXTURE)
+
+
+def _run(kernel):
+    sc = scenarios.c1()
+    d = tempfile.mkdtemp()
+    scenarios.write_inputs(sc, d)
+    cgfdm.run_directory(d, cgfdm.FP32, kernel)
+    return scenarios.read_outputs(sc, os.path.join(d, sc["params"]["out"]))
+
+
+def test_c1_exact_kernel_bitwise(c1_ref):
+    got = _run(cgfdm.KERNEL_EXACT)
+    np.testing.assert_array_equal(got["station_wave"], c1_ref["out_station_wave"])
+    np.testing.assert_array_equal(got["pgv"], c1_ref["out_pgv"])
+    np.testing.assert_array_equal(got["freesurf"], c1_ref["out_freesurf"])
+
+
+def test_c1_streaming_kernel_within_1e5(c1_ref):
+    got = _run(cgfdm.KERNEL_AUTO)
+    for v in range(3):
+        err = rel_l2(got["station_wave"][:, :, v], c1_ref["out_station_wave"][:, :, v])
+        assert err <= 1e-5, (v, err)
+    assert rel_l2(got["freesurf"][-1], c1_ref["out_freesurf"][-1]) <= 1e-5
+    assert rel_l2(got["pgv"], c1_ref["out_pgv"]) <= 1e-5
