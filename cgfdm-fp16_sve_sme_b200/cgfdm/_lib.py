@@ -90,6 +90,9 @@ SIGNATURES = {
     "cgfdm_set_tile_rows": (C.c_int, [P, I32]),
     "cgfdm_set_graph": (C.c_int, [P, I32]),
     "cgfdm_inject_fault": (C.c_int, [P, I32]),
+    "cgfdm_checkpoint_bytes": (C.c_int, [P, C.POINTER(I64)]),
+    "cgfdm_checkpoint_save": (C.c_int, [P, P, I64]),
+    "cgfdm_checkpoint_load": (C.c_int, [P, P, I64]),
     "cgfdm_batch_create": (C.c_int, [P, I32, C.POINTER(P)]),
     "cgfdm_batch_run": (C.c_int, [P, I32, P]),
     "cgfdm_batch_set_graph": (C.c_int, [P, I32]),

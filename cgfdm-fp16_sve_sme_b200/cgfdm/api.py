@@ -108,6 +108,20 @@ class Simulation:
         check(lib().cgfdm_get_timing(self._h, _ptr(ms)))
         return ms
 
+    def checkpoint(self):
+        """The handle's state at the current step boundary (bytes)."""
+        n = C.c_int64()
+        check(lib().cgfdm_checkpoint_bytes(self._h, C.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        check(lib().cgfdm_checkpoint_save(self._h, _ptr(buf), n.value))
+        return buf
+
+    def restore(self, buf):
+        """Continue from a checkpoint of a handle with the same descriptor,
+        sources and stations."""
+        buf = np.ascontiguousarray(buf, np.uint8)
+        check(lib().cgfdm_checkpoint_load(self._h, _ptr(buf), buf.size))
+
     def inject_fault(self, kind=1):
         """Failure-detection tests: the next streaming launch leaves one load
         unissued so that a bounded device wait expires (CGFDM_ERR_TIMEOUT)."""

@@ -186,6 +186,25 @@ int cgfdm_get_timing(cgfdm_handle *h, float *ms3) {
   return h->eng->get_timing(ms3);
 }
 
+int cgfdm_checkpoint_bytes(cgfdm_handle *h, int64_t *bytes) {
+  H_OR_FAIL(h);
+  if (!bytes) return CGFDM_ERR_ARG;
+  *bytes = h->eng->checkpoint_bytes();
+  return CGFDM_OK;
+}
+
+int cgfdm_checkpoint_save(cgfdm_handle *h, void *buf, int64_t bytes) {
+  H_OR_FAIL(h);
+  if (!buf) return CGFDM_ERR_ARG;
+  return h->eng->checkpoint_save(buf, bytes);
+}
+
+int cgfdm_checkpoint_load(cgfdm_handle *h, const void *buf, int64_t bytes) {
+  H_OR_FAIL(h);
+  if (!buf) return CGFDM_ERR_ARG;
+  return h->eng->checkpoint_load(buf, bytes);
+}
+
 int cgfdm_inject_fault(cgfdm_handle *h, int32_t kind) {
   H_OR_FAIL(h);
   return h->eng->inject_fault(kind);

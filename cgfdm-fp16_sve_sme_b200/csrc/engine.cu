@@ -460,6 +460,76 @@ template <typename S> class EngineT : public Engine {
 
   int get_wavefield(float *w) override { return download_repacked(A_, w, 9); }
 
+  // Checkpoint at a step boundary, raw device contents: a header, the three
+  // stage buffers A, X, Y (A is the step state; X and Y keep point-source
+  // values in their halo cells), the step-start PML auxiliaries, the PGV map,
+  // the seismograms and the step counter.  T and the other auxiliary buffers
+  // are rewritten by the next stage 0 before they are read.
+  struct CkptHeader {
+    char magic[8];
+    int32_t precision, nx, ny, nz, npml, nt, nsta, it;
+    int64_t wave_bytes, aux_bytes, pgv_bytes, sta_bytes;
+  };
+  int64_t checkpoint_bytes() const override {
+    return (int64_t)sizeof(CkptHeader) + 3 * wave_bytes() + aux_bytes() + pgv_bytes() +
+           sta_bytes();
+  }
+  int checkpoint_save(void *buf, int64_t bytes) override {
+    if (bytes < checkpoint_bytes()) {
+      set_error("checkpoint buffer too small");
+      return CGFDM_ERR_ARG;
+    }
+    int rc = synchronize();
+    if (rc) return rc;
+    CkptHeader h = header();
+    unsigned char *p = (unsigned char *)buf;
+    std::memcpy(p, &h, sizeof h);
+    p += sizeof h;
+    for (S *w : {A_, X_, Y_}) {
+      CUDA_TRY(cudaMemcpy(p, w, wave_bytes(), cudaMemcpyDeviceToHost));
+      p += wave_bytes();
+    }
+    if (aux_bytes()) CUDA_TRY(cudaMemcpy(p, auxbuf(0), aux_bytes(), cudaMemcpyDeviceToHost));
+    p += aux_bytes();
+    CUDA_TRY(cudaMemcpy(p, pgv_, pgv_bytes(), cudaMemcpyDeviceToHost));
+    p += pgv_bytes();
+    if (sta_bytes()) CUDA_TRY(cudaMemcpy(p, sta_wave_, sta_bytes(), cudaMemcpyDeviceToHost));
+    return CGFDM_OK;
+  }
+  int checkpoint_load(const void *buf, int64_t bytes) override {
+    CUDA_TRY(cudaSetDevice(d_.device));
+    CkptHeader h;
+    if (bytes < (int64_t)sizeof h) {
+      set_error("checkpoint buffer too small");
+      return CGFDM_ERR_ARG;
+    }
+    std::memcpy(&h, buf, sizeof h);
+    const CkptHeader mine = header();
+    if (std::memcmp(h.magic, mine.magic, 8) || h.precision != mine.precision || h.nx != mine.nx ||
+        h.ny != mine.ny || h.nz != mine.nz || h.npml != mine.npml || h.nt != mine.nt ||
+        h.nsta != mine.nsta || h.wave_bytes != mine.wave_bytes || h.aux_bytes != mine.aux_bytes ||
+        h.it < 0 || h.it > d_.nt || bytes < checkpoint_bytes()) {
+      set_error("checkpoint does not match this handle (grid, precision, nt or stations)");
+      return CGFDM_ERR_STATE;
+    }
+    int rc = synchronize();
+    if (rc) return rc;
+    const unsigned char *p = (const unsigned char *)buf + sizeof h;
+    for (S *w : {A_, X_, Y_}) {
+      CUDA_TRY(h2d(w, p, wave_bytes()));
+      p += wave_bytes();
+    }
+    if (aux_bytes()) CUDA_TRY(h2d(auxbuf(0), p, aux_bytes()));
+    p += aux_bytes();
+    CUDA_TRY(h2d(pgv_, p, pgv_bytes()));
+    p += pgv_bytes();
+    if (sta_bytes()) CUDA_TRY(h2d(sta_wave_, p, sta_bytes()));
+    it_ = h.it;
+    CUDA_TRY(h2d(step_, &h.it, sizeof(int)));
+    drop_graphs();
+    return CGFDM_OK;
+  }
+
   int get_free_surface(float *v3) override {
     const size_t n = (size_t)g_.nx * g_.ny;
     for (int v = 0; v < 3; ++v) {
@@ -621,6 +691,19 @@ template <typename S> class EngineT : public Engine {
 
  private:
   R *auxbuf(int b) const { return aux_ + (size_t)b * aux_total_; }
+  int64_t wave_bytes() const { return (int64_t)sizeof(S) * 9 * g_.L.fs; }
+  int64_t aux_bytes() const { return (int64_t)sizeof(R) * aux_total_; }
+  int64_t pgv_bytes() const { return (int64_t)sizeof(float) * 2 * g_.nx * g_.ny; }
+  int64_t sta_bytes() const { return (int64_t)sizeof(float) * nsta_ * d_.nt * 9; }
+  CkptHeader header() const {
+    CkptHeader h{};
+    std::memcpy(h.magic, "CGFDMCK1", 8);
+    h.precision = d_.precision; h.nx = d_.nx; h.ny = d_.ny; h.nz = d_.nz; h.npml = d_.npml;
+    h.nt = d_.nt; h.nsta = nsta_; h.it = it_;
+    h.wave_bytes = wave_bytes(); h.aux_bytes = aux_bytes(); h.pgv_bytes = pgv_bytes();
+    h.sta_bytes = sta_bytes();
+    return h;
+  }
 
   // Host-to-device copy ordered on the handle's stream and complete on
   // return (a plain cudaMemcpy from pageable memory may return before its

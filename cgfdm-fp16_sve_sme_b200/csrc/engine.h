@@ -47,6 +47,9 @@ class Engine {
   virtual int set_tile_rows(int rows) = 0;
   virtual int set_graph(bool on) = 0;
   virtual int inject_fault(int kind) = 0;
+  virtual int64_t checkpoint_bytes() const = 0;
+  virtual int checkpoint_save(void *buf, int64_t bytes) = 0;
+  virtual int checkpoint_load(const void *buf, int64_t bytes) = 0;
   virtual const cgfdm_desc &desc() const = 0;
 };
 

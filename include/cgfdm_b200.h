@@ -174,6 +174,17 @@ int cgfdm_get_kernel_stats(cgfdm_handle *h, double *out8);
  * choice is cached per (precision, grid) for the process. */
 int cgfdm_set_tile_rows(cgfdm_handle *h, int32_t rows);
 
+/* Checkpoint / resume at a step boundary (no counterpart in the reference):
+ * the handle's raw device state -- step wavefield, the two other stage
+ * buffers (their halo cells hold point-source values), step-start PML
+ * auxiliaries, PGV map, seismograms so far and the step counter -- into a
+ * host buffer of cgfdm_checkpoint_bytes bytes.  Loading it into a handle
+ * created with the same descriptor, sources and stations continues the run
+ * bit for bit.  The layout is this library's own (header "CGFDMCK1"). */
+int cgfdm_checkpoint_bytes(cgfdm_handle *h, int64_t *bytes);
+int cgfdm_checkpoint_save(cgfdm_handle *h, void *buf, int64_t bytes);
+int cgfdm_checkpoint_load(cgfdm_handle *h, const void *buf, int64_t bytes);
+
 /* Failure-detection testing (no counterpart in the reference): kind 1 makes
  * the next streaming-kernel launch of the handle leave one tile-plane load
  * unissued, so that one CTA's bounded wait expires (about 2^31 clock cycles,
