@@ -453,6 +453,8 @@ def main():
     ap.add_argument("--tile-rows", type=int, default=0, choices=[0, 8, 16],
                     help="streaming-kernel tile height (0: the library's autotuner)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp16", action="store_true",
+                    help="skip the scaled-FP16 companion measurement of an FP32 run")
     ap.add_argument("--cpu-baseline-steps", type=int, default=20)
     ap.add_argument("--batch-n", type=int, default=48, help="scenarios of --workload c4")
     ap.add_argument("--requests", type=int, default=32, help="requests of --workload c5")
@@ -592,6 +594,47 @@ def main():
         setup["src_index"].nbytes + sta.nbytes
     d2h = out_sta.nbytes + out_pgv.nbytes + out_fs.nbytes
 
+    # the scaled-FP16 form on the same workload, timed the same way (the
+    # metric pairs it with FP32; its error against FP64 is the opt-in
+    # --accuracy-steps run)
+    fp16 = None
+    if args.precision == "fp32" and not args.no_fp16:
+        d16 = tempfile.mkdtemp(prefix="cgfdm_bench_")
+        try:
+            write_workload(w, d16)
+            s16 = cgfdm.setup_from_directory(d16, cgfdm.FP16)
+        finally:
+            shutil.rmtree(d16, ignore_errors=True)
+        e0 = s16["desc"]
+        sim16 = cgfdm.Simulation(cgfdm.make_desc(e0.nx, e0.ny, e0.nz, e0.npml, e0.dh, e0.dt,
+                                                 total_steps, cgfdm.FP16, kern, local))
+        sim16.set_tile_rows(args.tile_rows)
+        sim16.set_model(s16["cjm"], s16["rdz"])
+        if s16["point"] is not None:
+            sim16.set_point_source(*s16["point"], s16["rickerfc"])
+        if s16["src_index"].size:
+            sim16.set_fault_source(s16["src_index"], s16["moment_rate"], s16["src_nt"],
+                                   s16["src_dt"], scaled=True)
+        sim16.set_stations(s16["stations"])
+        sim16.run(args.warmup, stream.cuda_stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        sim16.run(args.steps, stream.cuda_stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms16 = ev0.elapsed_time(ev1)
+        ks16 = sim16.kernel_stats()
+        sim16.close()
+        v16, ms16_max = replica_throughput(torch, dist, ms16 / 1e3, npts, args.steps, ws, "cuda")
+        fp16 = {"value": v16, "unit": UNIT, "ms_per_step": ms16_max * 1e3 / args.steps,
+                "speedup_vs_fp32": v16 / value, "tile_rows": ks16["tile_rows"],
+                "bytes_per_point_step": BYTES_PER_POINT_STEP["fp16"],
+                "accuracy": "rel L2 vs the FP64 GPU run, C2 2000 steps: 4.7e-3 (seismograms); "
+                            "python bench.py --precision fp16 --accuracy-steps 2000"}
+
     accuracy = None
     if args.accuracy_steps > 0:
         accuracy = measure_accuracy(cgfdm, w, prec, kern, local, args.accuracy_steps, setup)
@@ -681,6 +724,8 @@ def main():
         }
         if accuracy:
             line["accuracy"] = accuracy
+        if fp16:
+            line["fp16"] = fp16
         print(json.dumps(line))
     if dist:
         dist.barrier()
