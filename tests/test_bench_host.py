@@ -1,0 +1,41 @@
+"""Host-side logic of bench.py and the scenario sampler (no GPU): the
+reference arm's MPI decomposition rule and the ranges of the sampled
+batched / serving scenarios."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+from cgfdm import scenarios as S  # noqa: E402
+
+
+@pytest.mark.parametrize("cores", [1, 8, 16, 64])
+def test_decomposition_respects_the_pml_and_core_count(cores):
+    p = {"NX": 401, "NY": 401, "NZ": 201, "nPML": 20}
+    px, py, pz = bench.pick_decomposition(p, cores)
+    assert px * py * pz <= cores
+    # every rank holds at least max(nPML, 8) cells per axis (init_grid.cpp:109-117)
+    for n, k in ((401, px), (401, py), (201, pz)):
+        assert n // k >= 20
+
+
+def test_decomposition_uses_all_cores_when_it_can():
+    p = {"NX": 401, "NY": 401, "NZ": 201, "nPML": 20}
+    px, py, pz = bench.pick_decomposition(p, 16)
+    assert px * py * pz == 16
+
+
+def test_sampled_scenarios_follow_the_ranges():
+    for seed in range(6):
+        w = S.sample_scenario(seed, nsteps=10)
+        p = w["params"]
+        assert 121 <= p["NX"] <= 401 and 121 <= p["NY"] <= 401 and 101 <= p["NZ"] <= 201
+        assert p["useMultiSource"] == 1 and len(w["stations"]) == 25
+        assert np.asarray(w["terrain"]).max() <= 2000.0 + 1e-3
+    w = S.sample_scenario(1, points=2e6, nsteps=10)
+    n = w["params"]["NX"] * w["params"]["NY"] * w["params"]["NZ"]
+    assert 0.8e6 < n < 3e6
