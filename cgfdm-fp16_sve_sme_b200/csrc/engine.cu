@@ -136,8 +136,11 @@ template <typename S> class EngineT : public Engine {
     // both x1 and x2) are left to the exact-order kernel, which applies every
     // slab of a point; the streaming kernel applies one slab per axis
     const bool overlap = g_.npml > 0 && (2 * g_.npml > g_.nx || 2 * g_.npml > g_.ny);
+    // it also addresses a slab's auxiliaries with 32-bit offsets (9 x points < 2^32)
+    bool slabs_fit = true;
+    for (int s = 0; s < 5; ++s) slabs_fit = slabs_fit && 9 * g_.slab_pts[s] < (1LL << 32);
     use_stream_ = stage_stream_supported<S>() && d_.kernel != CGFDM_KERNEL_EXACT &&
-                  g_.nz > 3 && !overlap;
+                  g_.nz > 3 && !overlap && slabs_fit;
     if (d_.kernel == CGFDM_KERNEL_STREAM && !stage_stream_supported<S>() ) {
       set_error("the streaming kernel does not support this precision");
       return CGFDM_ERR_ARG;

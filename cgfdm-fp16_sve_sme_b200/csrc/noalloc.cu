@@ -30,6 +30,7 @@
 // first call before any stream capture.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -97,7 +98,7 @@ int stage_noalloc(const cgfdm_stage_buffers &b, cudaStream_t st, unsigned char *
   // PML slabs x1 y1 z1 x2 y2 (no top z slab), each field-major [9][pos] with
   // pos x-fastest inside the slab, concatenated in that order
   a.nslab = b.npml > 0 ? 5 : 0;
-  long long off = 0;
+  long long off = 0, big = 0;  // big: the largest slab's 9 x points
   for (int s = 0; s < a.nslab; ++s) {
     const int ax = s % 3, far = s >= 3;
     int n[3] = {b.nx, b.ny, b.nz}, o[3] = {HALO, HALO, HALO};
@@ -113,6 +114,7 @@ int stage_noalloc(const cgfdm_stage_buffers &b, cudaStream_t st, unsigned char *
     sl.am = b.aux_m + off;
     sl.at = b.aux_t + off;
     off += 9LL * n[0] * n[1] * n[2];
+    big = std::max(big, 9LL * n[0] * n[1] * n[2]);
   }
   // the profile table is rewritten by every call (host copy is staged by the
   // runtime before cudaMemcpyAsync returns, so the vector may go out of scope)
@@ -124,8 +126,9 @@ int stage_noalloc(const cgfdm_stage_buffers &b, cudaStream_t st, unsigned char *
   if (rc) return rc;
   int *err = (int *)scratch, *counter = (int *)(scratch + 4);
   // as a handle does: the exact-order kernel alone when opposite PML slabs
-  // overlap (nPML above half the grid)
-  const bool overlap = b.npml > 0 && (2 * b.npml > b.nx || 2 * b.npml > b.ny);
+  // overlap (nPML above half the grid) or a slab is too large for the
+  // streaming kernel's 32-bit auxiliary offsets
+  const bool overlap = b.npml > 0 && (2 * b.npml > b.nx || 2 * b.npml > b.ny || big >= (1LL << 32));
   const int ksurf = overlap ? HALO : L.nz_ - HALO - 3;
   StageArgs<S> lower = a;
   lower.kbeg = HALO;

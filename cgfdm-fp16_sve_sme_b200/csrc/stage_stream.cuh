@@ -1,4 +1,6 @@
-// TMA-staged z-streaming fused RK stage (the fast path).
+// TMA-staged z-streaming fused RK stage (the fast path).  Included by one
+// translation unit per storage type (stage_stream_f32.cu, _f16.cu, _bf16.cu),
+// each instantiating its own kernels.
 //
 // Persistent CTAs (one 512-thread CTA per SM) pull work items from an atomic
 // queue; an item is a 32 x 16 column tile and a chunk of z planes, ordered so
@@ -30,6 +32,7 @@
 //
 // Every mbarrier wait is bounded (2^31 clock cycles); on expiry the CTA sets
 // the error flag, drains the copies it issued (again bounded) and returns.
+#pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -127,8 +130,8 @@ __device__ __forceinline__ void elastic9(const float m[3], const float L[9], flo
   E[8] = (m[2] * L[1] + m[1] * L[2]) * mu;
 }
 
-__device__ __forceinline__ long long slab_pos(const SlabDev<float> &sl, int i, int j, int k) {
-  return (i - sl.off0) + (long long)(j - sl.off1) * sl.n0 + (long long)(k - sl.off2) * sl.n0 * sl.n1;
+__device__ __forceinline__ unsigned slab_pos(const SlabDev<float> &sl, int i, int j, int k) {
+  return (unsigned)((i - sl.off0) + (j - sl.off1) * sl.n0 + (k - sl.off2) * sl.n0 * sl.n1);
 }
 
 // PML auxiliary update of one slab point (pml_deriv.cpp:199-237,
@@ -137,14 +140,15 @@ __device__ __forceinline__ long long slab_pos(const SlabDev<float> &sl, int i, i
 // (value v at v * np + pos), so the lanes of a warp, consecutive points of
 // the slab, touch consecutive addresses.  Fields go three at a time, each
 // group's loads issued before its stores (the buffers do not overlap).
-__device__ __forceinline__ void pml_point(const SlabDev<float> &sl, long long pos, const float E[9],
-                                          float dl, float ad, float bt, float DT, int irk,
-                                          float h[9]) {
-  const long long np = sl.np;
-  const float *__restrict__ ain = sl.ain + pos;
-  const float *__restrict__ am = sl.am + pos;
-  float *__restrict__ aout = sl.aout + pos;
-  float *__restrict__ at = sl.at + pos;
+template <int RK>
+__device__ __forceinline__ void pml_point(const SlabDev<float> &sl, unsigned pos, const float E[9],
+                                          float dl, float ad, float bt, float DT, float cB,
+                                          float cA, float h[9]) {
+  const unsigned np = (unsigned)sl.np;
+  const float *__restrict__ ain = sl.ain;
+  const float *__restrict__ am = sl.am;
+  float *__restrict__ aout = sl.aout;
+  float *__restrict__ at = sl.at;
   // three fields at a time: their auxiliary input, what the stage adds the
   // increment to (m in stages 1-2, t in stage 3) and t itself (stages 1-2)
 #pragma unroll
@@ -152,33 +156,26 @@ __device__ __forceinline__ void pml_point(const SlabDev<float> &sl, long long po
     float av[3], bv[3], tv[3];
 #pragma unroll
     for (int u = 0; u < 3; ++u) {
-      const long long q = (g + u) * np;
+      const unsigned q = (g + u) * np + pos;
       av[u] = ain[q];
-      bv[u] = irk == 0 ? 0.0f : irk == 3 ? at[q] : am[q];
-      tv[u] = (irk == 1 || irk == 2) ? at[q] : 0.0f;
+      bv[u] = RK == 0 ? 0.0f : RK == 3 ? at[q] : am[q];
+      tv[u] = RK == 1 ? at[q] : 0.0f;
     }
 #pragma unroll
     for (int u = 0; u < 3; ++u) {
       const int v = g + u;
-      const long long q = v * np;
+      const unsigned q = v * np + pos;
       const float a = av[u];
       const float ha = (dl * E[v] - ad * a) * DT;
       h[v] -= bt * a * DT;
-      switch (irk) {
-        case 0:
-          at[q] = a + kB1 * ha;
-          aout[q] = a + kA2rk * ha;
-          break;
-        case 1:
-          at[q] = tv[u] + kB2 * ha;
-          aout[q] = bv[u] + kA3rk * ha;
-          break;
-        case 2:
-          at[q] = tv[u] + kB3 * ha;
-          aout[q] = bv[u] + ha;
-          break;
-        default:
-          aout[q] = bv[u] + kB4 * ha;
+      if (RK == 0) {
+        at[q] = a + kB1 * ha;
+        aout[q] = a + kA2rk * ha;
+      } else if (RK == 1) {
+        at[q] = tv[u] + cB * ha;
+        aout[q] = bv[u] + cA * ha;
+      } else {
+        aout[q] = bv[u] + kB4 * ha;
       }
     }
   }
@@ -302,7 +299,7 @@ template <typename S> struct BatchSrc {
   __device__ const Work &work(int e) const { return p.work[e]; }
 };
 
-template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK, typename Src>
+template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK, int RK, typename Src>
 __device__ __forceinline__ void stream_body(const Src &src, int *err) {
   using G = Geo<S, TYv>;
   constexpr int TY = G::TY, NTHR = G::NTHR, BY = G::BY;
@@ -340,8 +337,9 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
     const Maps &maps = src.maps(e);
     const Work &wk = src.work(e);
     const Layout L = a.L;
-    const int irk = a.irk;
-    const bool need_m = irk == 1 || irk == 2, need_t = irk >= 1;
+    // stages 1 and 2 (RK = 1) differ only in the weights of the t and output updates
+    constexpr bool need_m = RK == 1, need_t = RK >= 1;
+    const float cB = a.irk == 2 ? kB3 : kB2, cA = a.irk == 2 ? 1.0f : kA3rk;
     const uint32_t m_bytes = (need_m ? 9 : 0) * NTHR * G::ES + (need_t ? 9 : 0) * NTHR * G::ES;
     const float rDH = a.rDH, DT = a.DT;
     // stencil weights with the MacCormack sign and 1/DH folded in
@@ -404,6 +402,9 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
       sx = i < HALO + np ? 0 : i >= L.nx_ - HALO - np ? 3 : -1;
       sy = j < HALO + np ? 1 : j >= L.ny_ - HALO - np ? 4 : -1;
     }
+    float dlx = 0.f, btx = 0.f, adx = 0.f, dly = 0.f, bty = 0.f, ady = 0.f;
+    if (PMLK && sx >= 0) { dlx = __ldg(px + 2 * L.nx_ + i); btx = __ldg(px + L.nx_ + i); adx = __ldg(px + i) + dlx; }
+    if (PMLK && sy >= 0) { dly = __ldg(py + 2 * L.ny_ + j); bty = __ldg(py + L.ny_ + j); ady = __ldg(py + j) + dly; }
 
     // z window in registers: physical slot n mod 5 holds input plane q_n; the
     // plane loop is unrolled five times so that every slot index is a
@@ -446,7 +447,7 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         }
         const float mu = ldv(cf + 9 * NTHR + cidx), lam = ldv(cf + 10 * NTHR + cidx);
         const float bu = ldv(cf + 11 * NTHR + cidx) * (float)CRHO_OF<S>::v;
-        const float bzd = pz[L.nz_ + k] * DT;
+        const float bzd = __ldg(pz + L.nz_ + k) * DT;
         float h[9], Lr[9], E[9];
         // x direction
 #pragma unroll
@@ -459,8 +460,7 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
 #pragma unroll
         for (int v = 0; v < 9; ++v) h[v] = bxd * E[v];
         if (PMLK && sx >= 0) {  // profile values d, alpha + d, beta at this x
-          const float dl = px[2 * L.nx_ + i], bt = px[L.nx_ + i], ad = px[i] + dl;
-          pml_point(a.slab[sx], slab_pos(a.slab[sx], i, j, k), E, dl, ad, bt, DT, irk, h);
+          pml_point<RK>(a.slab[sx], slab_pos(a.slab[sx], i, j, k), E, dlx, adx, btx, DT, cB, cA, h);
         }
         // y direction
 #pragma unroll
@@ -473,8 +473,7 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
 #pragma unroll
         for (int v = 0; v < 9; ++v) h[v] += byd * E[v];
         if (PMLK && sy >= 0) {
-          const float dl = py[2 * L.ny_ + j], bt = py[L.ny_ + j], ad = py[j] + dl;
-          pml_point(a.slab[sy], slab_pos(a.slab[sy], i, j, k), E, dl, ad, bt, DT, irk, h);
+          pml_point<RK>(a.slab[sy], slab_pos(a.slab[sy], i, j, k), E, dly, ady, bty, DT, cB, cA, h);
         }
         // z direction: W[k - m*DIR] for m = -1..3 sits in slots P0 (q = k + DIR) .. P4
 #pragma unroll
@@ -485,8 +484,8 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
 #pragma unroll
         for (int v = 0; v < 9; ++v) h[v] += bzd * E[v];
         if (PMLK && a.nslab && k < HALO + a.npml) {
-          const float dlz = pz[2 * L.nz_ + k], btz = pz[L.nz_ + k], adz = pz[k] + dlz;
-          pml_point(a.slab[2], slab_pos(a.slab[2], i, j, k), E, dlz, adz, btz, DT, irk, h);
+          const float dlz = __ldg(pz + 2 * L.nz_ + k), btz = __ldg(pz + L.nz_ + k), adz = __ldg(pz + k) + dlz;
+          pml_point<RK>(a.slab[2], slab_pos(a.slab[2], i, j, k), E, dlz, adz, btz, DT, cB, cA, h);
         }
         // RK4 combination (wave_rk.cpp:13-99)
         const S *ms = (const S *)(smem + G::OFF_M + ((fm0 + o) % NM) * G::M_BYTES);
@@ -496,22 +495,15 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         for (int v = 0; v < 9; ++v) {
           const float hv = h[v];
           const long long q = ctr + v * fs;
-          switch (irk) {
-            case 0: {
-              const float m0 = win[v][P1];  // the stage input at k is the step state
-              stv(a.t + q, m0 + kB1 * hv);
-              stv(a.wout + q, m0 + kA2rk * hv);
-            } break;
-            case 1:
-              stv(a.t + q, ldv(ts + v * NTHR + cidx) + kB2 * hv);
-              stv(a.wout + q, ldv(ms + v * NTHR + cidx) + kA3rk * hv);
-              break;
-            case 2:
-              stv(a.t + q, ldv(ts + v * NTHR + cidx) + kB3 * hv);
-              stv(a.wout + q, ldv(ms + v * NTHR + cidx) + hv);
-              break;
-            default:
-              stv(a.wout + q, ldv(ts + v * NTHR + cidx) + kB4 * hv);
+          if (RK == 0) {
+            const float m0 = win[v][P1];  // the stage input at k is the step state
+            stv(a.t + q, m0 + kB1 * hv);
+            stv(a.wout + q, m0 + kA2rk * hv);
+          } else if (RK == 1) {
+            stv(a.t + q, ldv(ts + v * NTHR + cidx) + cB * hv);
+            stv(a.wout + q, ldv(ms + v * NTHR + cidx) + cA * hv);
+          } else {
+            stv(a.wout + q, ldv(ts + v * NTHR + cidx) + kB4 * hv);
           }
         }
       }
@@ -571,25 +563,25 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
   }
 }
 
-template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK>
+template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK, int RK>
 __global__ void __launch_bounds__(TX * TYv, Geo<S, TYv>::MINB)
     stage_stream_kernel(const __grid_constant__ Maps maps, const __grid_constant__ StageArgs<S> a,
                         const __grid_constant__ Work wk, int *err) {
-  stream_body<S, TYv, FB1, FB2, FB3, PMLK>(SingleSrc<S>{maps, a, wk}, err);
+  stream_body<S, TYv, FB1, FB2, FB3, PMLK, RK>(SingleSrc<S>{maps, a, wk}, err);
 }
 
-template <typename S, int FB1, int FB2, int FB3, bool PMLK>
+template <typename S, int FB1, int FB2, int FB3, bool PMLK, int RK>
 __global__ void __launch_bounds__(TX * 16, 1)
     stage_stream_batch_kernel(const __grid_constant__ BatchParams<S> p, int *err) {
-  stream_body<S, 16, FB1, FB2, FB3, PMLK>(BatchSrc<S>{p}, err);
+  stream_body<S, 16, FB1, FB2, FB3, PMLK, RK>(BatchSrc<S>{p}, err);
 }
 
-template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK>
+template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK, int RK>
 cudaError_t launch_variant(const StageArgs<S> &a, const Maps &maps, const Work &wk, int *err,
                            int nsm, cudaStream_t st) {
   using G = Geo<S, TYv>;
   static int attr_dev = -1;
-  auto kern = stage_stream_kernel<S, TYv, FB1, FB2, FB3, PMLK>;
+  auto kern = stage_stream_kernel<S, TYv, FB1, FB2, FB3, PMLK, RK>;
   const int smem = G::SMEM;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -659,7 +651,7 @@ WorkPlan plan_work(const StageArgs<S> &a, int nsm, int *counter) {
 
 // Splits the stage into the interior launch (tiles and chunks that touch no
 // PML slab) and the PML launch (the rest), see Work.
-template <typename S, int TYv, int FB1, int FB2, int FB3>
+template <typename S, int TYv, int FB1, int FB2, int FB3, int RK>
 cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *counter,
                        cudaStream_t st, int *nlaunch) {
   const int nsm = sm_count();
@@ -668,27 +660,27 @@ cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *c
   Work wi = wp.wk;
   wi.nitems = wp.n_in;
   if (wi.nitems > 0) {
-    e = launch_variant<S, TYv, FB1, FB2, FB3, false>(a, maps, wi, err, nsm, st);
+    e = launch_variant<S, TYv, FB1, FB2, FB3, false, RK>(a, maps, wi, err, nsm, st);
     if (e != cudaSuccess) return e;
     if (nlaunch) ++*nlaunch;
   }
   Work wq = wp.wk;
   wq.nitems = wp.n_pml;
   if (wq.nitems > 0) {
-    e = launch_variant<S, TYv, FB1, FB2, FB3, true>(a, maps, wq, err, nsm, st);
+    e = launch_variant<S, TYv, FB1, FB2, FB3, true, RK>(a, maps, wq, err, nsm, st);
     if (e != cudaSuccess) return e;
     if (nlaunch) ++*nlaunch;
   }
   return cudaSuccess;
 }
 
-template <typename S, int FB1, int FB2, int FB3, bool PMLK>
+template <typename S, int FB1, int FB2, int FB3, bool PMLK, int RK>
 cudaError_t launch_batch_variant(const BatchParams<S> &p, int items, int *err, int nsm,
                                  cudaStream_t st) {
   using G = Geo<S, 16>;
   static_assert(sizeof(BatchParams<S>) <= 32000, "kernel parameter space");
   static int attr_dev = -1;
-  auto kern = stage_stream_batch_kernel<S, FB1, FB2, FB3, PMLK>;
+  auto kern = stage_stream_batch_kernel<S, FB1, FB2, FB3, PMLK, RK>;
   const int smem = G::SMEM;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -706,7 +698,7 @@ cudaError_t launch_batch_variant(const BatchParams<S> &p, int items, int *err, i
 
 // One stage of n scenarios that share the MacCormack signs: kBatchMax
 // scenarios per launch pair (interior items of all of them, then PML items).
-template <typename S, int FB1, int FB2, int FB3>
+template <typename S, int FB1, int FB2, int FB3, int RK>
 cudaError_t launch_batch(const StageArgs<S> *args, const void *const *maps, int n, int *err,
                          int *counter, cudaStream_t st, int *nlaunch) {
   const int nsm = sm_count();
@@ -736,8 +728,8 @@ cudaError_t launch_batch(const StageArgs<S> *args, const void *const *maps, int 
       bp->n = m;
       bp->counter = counter;
       cudaError_t e = pass == 0
-                          ? launch_batch_variant<S, FB1, FB2, FB3, false>(*bp, total, err, nsm, st)
-                          : launch_batch_variant<S, FB1, FB2, FB3, true>(*bp, total, err, nsm, st);
+                          ? launch_batch_variant<S, FB1, FB2, FB3, false, RK>(*bp, total, err, nsm, st)
+                          : launch_batch_variant<S, FB1, FB2, FB3, true, RK>(*bp, total, err, nsm, st);
       if (e != cudaSuccess) return e;
       if (nlaunch) ++*nlaunch;
     }
@@ -793,7 +785,17 @@ int encode_map(const S *base, const Layout &L, int nfield, int bx, int by, int b
 }  // namespace
 
 template <typename S> bool stage_stream_supported() { return true; }
-template <> bool stage_stream_supported<double>() { return false; }
+// FP64 has none (stage_stream_f32.cu defines these specialisations)
+template <> bool stage_stream_supported<double>();
+template <>
+int encode_stream_maps<double>(const double *, const double *, const double *, const double *,
+                               const Layout &, void *);
+template <>
+cudaError_t launch_stage_stream_batch<double>(const StageArgs<double> *, const void *const *, int,
+                                              int *, int *, cudaStream_t, int *);
+template <>
+cudaError_t launch_stage_stream<double>(const StageArgs<double> &, const void *, int *, int *,
+                                        cudaStream_t, cudaEvent_t, int *, int);
 
 template <typename S>
 int encode_stream_maps(const S *wave, const S *cjm, const S *wm, const S *t, const Layout &L,
@@ -812,26 +814,48 @@ int encode_stream_maps(const S *wave, const S *cjm, const S *wm, const S *t, con
   if (!rc) std::memcpy(out, &ms, sizeof ms);
   return rc;
 }
-template <>
-int encode_stream_maps<double>(const double *, const double *, const double *, const double *,
-                               const Layout &, void *) {
-  set_error("no streaming kernel for FP64");
-  return CGFDM_ERR_ARG;
-}
 
+// The stage class RK of stage irk: 0, 1 (stages 1 and 2) or 3.
+inline int rk_class(int irk) { return irk == 0 ? 0 : irk == 3 ? 3 : 1; }
+
+template <typename S, int TYv, int RK>
+cudaError_t launch_fb_rk(const StageArgs<S> &a, const Maps &m, int *err, int *counter,
+                         cudaStream_t st, int *nlaunch) {
+  const int code = (a.fb1 > 0) * 4 + (a.fb2 > 0) * 2 + (a.fb3 > 0);
+  switch (code) {
+    case 0: return launch_one<S, TYv, -1, -1, -1, RK>(a, m, err, counter, st, nlaunch);
+    case 1: return launch_one<S, TYv, -1, -1, 1, RK>(a, m, err, counter, st, nlaunch);
+    case 2: return launch_one<S, TYv, -1, 1, -1, RK>(a, m, err, counter, st, nlaunch);
+    case 3: return launch_one<S, TYv, -1, 1, 1, RK>(a, m, err, counter, st, nlaunch);
+    case 4: return launch_one<S, TYv, 1, -1, -1, RK>(a, m, err, counter, st, nlaunch);
+    case 5: return launch_one<S, TYv, 1, -1, 1, RK>(a, m, err, counter, st, nlaunch);
+    case 6: return launch_one<S, TYv, 1, 1, -1, RK>(a, m, err, counter, st, nlaunch);
+    default: return launch_one<S, TYv, 1, 1, 1, RK>(a, m, err, counter, st, nlaunch);
+  }
+}
 template <typename S, int TYv>
 cudaError_t launch_fb(const StageArgs<S> &a, const Maps &m, int *err, int *counter,
                       cudaStream_t st, int *nlaunch) {
-  const int code = (a.fb1 > 0) * 4 + (a.fb2 > 0) * 2 + (a.fb3 > 0);
-  switch (code) {
-    case 0: return launch_one<S, TYv, -1, -1, -1>(a, m, err, counter, st, nlaunch);
-    case 1: return launch_one<S, TYv, -1, -1, 1>(a, m, err, counter, st, nlaunch);
-    case 2: return launch_one<S, TYv, -1, 1, -1>(a, m, err, counter, st, nlaunch);
-    case 3: return launch_one<S, TYv, -1, 1, 1>(a, m, err, counter, st, nlaunch);
-    case 4: return launch_one<S, TYv, 1, -1, -1>(a, m, err, counter, st, nlaunch);
-    case 5: return launch_one<S, TYv, 1, -1, 1>(a, m, err, counter, st, nlaunch);
-    case 6: return launch_one<S, TYv, 1, 1, -1>(a, m, err, counter, st, nlaunch);
-    default: return launch_one<S, TYv, 1, 1, 1>(a, m, err, counter, st, nlaunch);
+  switch (rk_class(a.irk)) {
+    case 0: return launch_fb_rk<S, TYv, 0>(a, m, err, counter, st, nlaunch);
+    case 1: return launch_fb_rk<S, TYv, 1>(a, m, err, counter, st, nlaunch);
+    default: return launch_fb_rk<S, TYv, 3>(a, m, err, counter, st, nlaunch);
+  }
+}
+
+template <typename S, int RK>
+cudaError_t launch_batch_rk(const StageArgs<S> *args, const void *const *maps, int n, int *err,
+                            int *counter, cudaStream_t st, int *nlaunch) {
+  const StageArgs<S> &a = args[0];
+  switch ((a.fb1 > 0) * 4 + (a.fb2 > 0) * 2 + (a.fb3 > 0)) {
+    case 0: return launch_batch<S, -1, -1, -1, RK>(args, maps, n, err, counter, st, nlaunch);
+    case 1: return launch_batch<S, -1, -1, 1, RK>(args, maps, n, err, counter, st, nlaunch);
+    case 2: return launch_batch<S, -1, 1, -1, RK>(args, maps, n, err, counter, st, nlaunch);
+    case 3: return launch_batch<S, -1, 1, 1, RK>(args, maps, n, err, counter, st, nlaunch);
+    case 4: return launch_batch<S, 1, -1, -1, RK>(args, maps, n, err, counter, st, nlaunch);
+    case 5: return launch_batch<S, 1, -1, 1, RK>(args, maps, n, err, counter, st, nlaunch);
+    case 6: return launch_batch<S, 1, 1, -1, RK>(args, maps, n, err, counter, st, nlaunch);
+    default: return launch_batch<S, 1, 1, 1, RK>(args, maps, n, err, counter, st, nlaunch);
   }
 }
 
@@ -858,54 +882,11 @@ cudaError_t launch_stage_stream_batch(const StageArgs<S> *args, const void *cons
     if (args[q].fb1 != args[0].fb1 || args[q].fb2 != args[0].fb2 || args[q].fb3 != args[0].fb3 ||
         args[q].irk != args[0].irk)
       return cudaErrorInvalidValue;
-  const StageArgs<S> &a = args[0];
-  switch ((a.fb1 > 0) * 4 + (a.fb2 > 0) * 2 + (a.fb3 > 0)) {
-    case 0: return launch_batch<S, -1, -1, -1>(args, maps, n, err, counter, st, nlaunch);
-    case 1: return launch_batch<S, -1, -1, 1>(args, maps, n, err, counter, st, nlaunch);
-    case 2: return launch_batch<S, -1, 1, -1>(args, maps, n, err, counter, st, nlaunch);
-    case 3: return launch_batch<S, -1, 1, 1>(args, maps, n, err, counter, st, nlaunch);
-    case 4: return launch_batch<S, 1, -1, -1>(args, maps, n, err, counter, st, nlaunch);
-    case 5: return launch_batch<S, 1, -1, 1>(args, maps, n, err, counter, st, nlaunch);
-    case 6: return launch_batch<S, 1, 1, -1>(args, maps, n, err, counter, st, nlaunch);
-    default: return launch_batch<S, 1, 1, 1>(args, maps, n, err, counter, st, nlaunch);
+  switch (rk_class(args[0].irk)) {
+    case 0: return launch_batch_rk<S, 0>(args, maps, n, err, counter, st, nlaunch);
+    case 1: return launch_batch_rk<S, 1>(args, maps, n, err, counter, st, nlaunch);
+    default: return launch_batch_rk<S, 3>(args, maps, n, err, counter, st, nlaunch);
   }
 }
-template <>
-cudaError_t launch_stage_stream_batch<double>(const StageArgs<double> *, const void *const *, int,
-                                              int *, int *, cudaStream_t, int *) {
-  return cudaErrorNotSupported;
-}
-
-template <>
-cudaError_t launch_stage_stream<double>(const StageArgs<double> &, const void *, int *, int *,
-                                        cudaStream_t, cudaEvent_t, int *, int) {
-  return cudaErrorNotSupported;
-}
-
-template cudaError_t launch_stage_stream_batch<float>(const StageArgs<float> *,
-                                                      const void *const *, int, int *, int *,
-                                                      cudaStream_t, int *);
-template cudaError_t launch_stage_stream_batch<__half>(const StageArgs<__half> *,
-                                                       const void *const *, int, int *, int *,
-                                                       cudaStream_t, int *);
-template cudaError_t launch_stage_stream_batch<__nv_bfloat16>(const StageArgs<__nv_bfloat16> *,
-                                                              const void *const *, int, int *,
-                                                              int *, cudaStream_t, int *);
-template bool stage_stream_supported<float>();
-template bool stage_stream_supported<__half>();
-template bool stage_stream_supported<__nv_bfloat16>();
-template int encode_stream_maps<float>(const float *, const float *, const float *, const float *,
-                                       const Layout &, void *);
-template int encode_stream_maps<__half>(const __half *, const __half *, const __half *,
-                                        const __half *, const Layout &, void *);
-template int encode_stream_maps<__nv_bfloat16>(const __nv_bfloat16 *, const __nv_bfloat16 *,
-                                               const __nv_bfloat16 *, const __nv_bfloat16 *,
-                                               const Layout &, void *);
-template cudaError_t launch_stage_stream<float>(const StageArgs<float> &, const void *, int *,
-                                                int *, cudaStream_t, cudaEvent_t, int *, int);
-template cudaError_t launch_stage_stream<__half>(const StageArgs<__half> &, const void *, int *,
-                                                 int *, cudaStream_t, cudaEvent_t, int *, int);
-template cudaError_t launch_stage_stream<__nv_bfloat16>(const StageArgs<__nv_bfloat16> &,
-                                                        const void *, int *, int *, cudaStream_t, cudaEvent_t, int *, int);
 
 }  // namespace cgfdm
