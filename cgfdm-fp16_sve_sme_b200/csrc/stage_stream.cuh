@@ -138,48 +138,67 @@ __device__ __forceinline__ unsigned slab_pos(const SlabDev<float> &sl, int i, in
 // pml_rk.cpp:15-69) given the direction's elastic combination E; adds
 // -beta * Aux * DT into h.  The auxiliaries are field-major on the device
 // (value v at v * np + pos), so the lanes of a warp, consecutive points of
-// the slab, touch consecutive addresses.  Fields go three at a time, each
-// group's loads issued before its stores (the buffers do not overlap).
-template <int RK>
-__device__ __forceinline__ void pml_point(const SlabDev<float> &sl, unsigned pos, const float E[9],
-                                          float dl, float ad, float bt, float DT, float cB,
-                                          float cA, float h[9]) {
+// the slab, touch consecutive addresses.
+//
+// A point's inputs are the auxiliary input (part 1), what the stage adds the
+// increment to (part 2: m in stages 1-2, t in stage 3) and t (part 4, stages
+// 1-2).  pml_load<RK, H> loads the parts in H for all nine fields, so that
+// the loads can be issued at the top of a plane iteration and their latency
+// overlaps the stencil work; pml_apply<RK, H> loads the other parts (three
+// fields at a time, each group's loads before its stores) and updates.
+template <int RK> constexpr int pml_parts() { return RK == 0 ? 1 : RK == 3 ? 3 : 7; }
+struct PmlIn {
+  float a[9], b[9], t[9];
+};
+template <int RK, int H>
+__device__ __forceinline__ void pml_load_fields(const SlabDev<float> &sl, unsigned pos, int v0,
+                                                int nv, PmlIn &in) {
+  constexpr int P = pml_parts<RK>() & H;
   const unsigned np = (unsigned)sl.np;
-  const float *__restrict__ ain = sl.ain;
-  const float *__restrict__ am = sl.am;
+#pragma unroll
+  for (int v = v0; v < v0 + nv; ++v) {
+    const unsigned q = v * np + pos;
+    if (P & 1) in.a[v] = sl.ain[q];
+    if (P & 2) in.b[v] = RK == 3 ? sl.at[q] : sl.am[q];
+    if (P & 4) in.t[v] = sl.at[q];
+  }
+}
+template <int RK, int H>
+__device__ __forceinline__ void pml_load(const SlabDev<float> &sl, unsigned pos, PmlIn &in) {
+  pml_load_fields<RK, H>(sl, pos, 0, 9, in);
+}
+template <int RK, int H>
+__device__ __forceinline__ void pml_apply(const SlabDev<float> &sl, unsigned pos, const float E[9],
+                                          float dl, float ad, float bt, float DT, float cB,
+                                          float cA, float h[9], PmlIn &in) {
+  const unsigned np = (unsigned)sl.np;
   float *__restrict__ aout = sl.aout;
   float *__restrict__ at = sl.at;
-  // three fields at a time: their auxiliary input, what the stage adds the
-  // increment to (m in stages 1-2, t in stage 3) and t itself (stages 1-2)
 #pragma unroll
   for (int g = 0; g < 9; g += 3) {
-    float av[3], bv[3], tv[3];
+    pml_load_fields<RK, 7 & ~H>(sl, pos, g, 3, in);
 #pragma unroll
-    for (int u = 0; u < 3; ++u) {
-      const unsigned q = (g + u) * np + pos;
-      av[u] = ain[q];
-      bv[u] = RK == 0 ? 0.0f : RK == 3 ? at[q] : am[q];
-      tv[u] = RK == 1 ? at[q] : 0.0f;
-    }
-#pragma unroll
-    for (int u = 0; u < 3; ++u) {
-      const int v = g + u;
+    for (int v = g; v < g + 3; ++v) {
       const unsigned q = v * np + pos;
-      const float a = av[u];
+      const float a = in.a[v];
       const float ha = (dl * E[v] - ad * a) * DT;
       h[v] -= bt * a * DT;
       if (RK == 0) {
         at[q] = a + kB1 * ha;
         aout[q] = a + kA2rk * ha;
       } else if (RK == 1) {
-        at[q] = tv[u] + cB * ha;
-        aout[q] = bv[u] + cA * ha;
+        at[q] = in.t[v] + cB * ha;
+        aout[q] = in.b[v] + cA * ha;
       } else {
-        aout[q] = bv[u] + kB4 * ha;
+        aout[q] = in.b[v] + kB4 * ha;
       }
     }
   }
 }
+// The parts of an x-slab point loaded at the top of its plane iteration:
+// all of them in stages 0 and 3; the auxiliary input alone in stages 1-2,
+// where holding all three parts (27 registers) across the stencils spills.
+template <int RK> constexpr int hoist_parts() { return RK == 1 ? 1 : pml_parts<RK>(); }
 
 struct Maps {
   CUtensorMap w;   // stage input wavefield, box BX x BY x 1 x 9
@@ -420,6 +439,11 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
       constexpr int R = decltype(Rc)::value;
       constexpr int P0 = R, P1 = (R + 4) % 5, P2 = (R + 3) % 5, P3 = (R + 2) % 5, P4 = (R + 1) % 5;
       const int o = n - 4;  // output index of this iteration (o < 0: window warm-up)
+      constexpr int HP = hoist_parts<RK>();
+      // the x-slab inputs of this plane's point, issued before the waits
+      PmlIn pin;
+      const int kk = q0 + n * DIR - DIR;
+      if (PMLK && o >= 0 && sx >= 0) pml_load<RK, HP>(a.slab[sx], slab_pos(a.slab[sx], i, j, kk), pin);
       bool ok = mbar_wait_bounded(smem_u32(&bw[(fw0 + n) % NW]), ((fw0 + n) / NW) & 1);
       if (o >= 0) {
         ok = ok && mbar_wait_bounded(smem_u32(&bc[(fc0 + o) % NC]), ((fc0 + o) / NC) & 1);
@@ -460,7 +484,7 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
 #pragma unroll
         for (int v = 0; v < 9; ++v) h[v] = bxd * E[v];
         if (PMLK && sx >= 0) {  // profile values d, alpha + d, beta at this x
-          pml_point<RK>(a.slab[sx], slab_pos(a.slab[sx], i, j, k), E, dlx, adx, btx, DT, cB, cA, h);
+          pml_apply<RK, HP>(a.slab[sx], slab_pos(a.slab[sx], i, j, k), E, dlx, adx, btx, DT, cB, cA, h, pin);
         }
         // y direction
 #pragma unroll
@@ -473,7 +497,8 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
 #pragma unroll
         for (int v = 0; v < 9; ++v) h[v] += byd * E[v];
         if (PMLK && sy >= 0) {
-          pml_point<RK>(a.slab[sy], slab_pos(a.slab[sy], i, j, k), E, dly, ady, bty, DT, cB, cA, h);
+          PmlIn late;
+          pml_apply<RK, 0>(a.slab[sy], slab_pos(a.slab[sy], i, j, k), E, dly, ady, bty, DT, cB, cA, h, late);
         }
         // z direction: W[k - m*DIR] for m = -1..3 sits in slots P0 (q = k + DIR) .. P4
 #pragma unroll
@@ -485,7 +510,8 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         for (int v = 0; v < 9; ++v) h[v] += bzd * E[v];
         if (PMLK && a.nslab && k < HALO + a.npml) {
           const float dlz = __ldg(pz + 2 * L.nz_ + k), btz = __ldg(pz + L.nz_ + k), adz = __ldg(pz + k) + dlz;
-          pml_point<RK>(a.slab[2], slab_pos(a.slab[2], i, j, k), E, dlz, adz, btz, DT, cB, cA, h);
+          PmlIn late;
+          pml_apply<RK, 0>(a.slab[2], slab_pos(a.slab[2], i, j, k), E, dlz, adz, btz, DT, cB, cA, h, late);
         }
         // RK4 combination (wave_rk.cpp:13-99)
         const S *ms = (const S *)(smem + G::OFF_M + ((fm0 + o) % NM) * G::M_BYTES);
