@@ -130,6 +130,27 @@ __device__ __forceinline__ void elastic9(const float m[3], const float L[9], flo
   E[8] = (m[2] * L[1] + m[1] * L[2]) * mu;
 }
 
+// Packed FP32x2 arithmetic (FFMA2 / FMUL2 on sm_100): one instruction applies
+// the same operation to two fields of a point, each lane rounding exactly as
+// the scalar operation would.
+__device__ __forceinline__ float2 pk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 pk(float a) { return make_float2(a, a); }
+
+// One-sided 5-point sum with the MacCormack weights as they stand
+// (macro.h:126-136), taps in the order (-FB, 0, +FB, +2FB, +3FB); the sign FB
+// and 1/DH multiply the direction's elastic combination afterwards (it is
+// linear in the derivatives).
+__device__ __forceinline__ float2 stencil2(float2 t0, float2 t1, float2 t2, float2 t3, float2 t4) {
+  float2 s = __fmul2_rn(pk(kAm1), t0);
+  s = __ffma2_rn(pk(kA0), t1, s);
+  s = __ffma2_rn(pk(kA1), t2, s);
+  s = __ffma2_rn(pk(kA2), t3, s);
+  return __ffma2_rn(pk(kA3), t4, s);
+}
+__device__ __forceinline__ float stencil1(float t0, float t1, float t2, float t3, float t4) {
+  return fmaf(kA3, t4, fmaf(kA2, t3, fmaf(kA1, t2, fmaf(kA0, t1, kAm1 * t0))));
+}
+
 __device__ __forceinline__ unsigned slab_pos(const SlabDev<float> &sl, int i, int j, int k) {
   return (unsigned)((i - sl.off0) + (j - sl.off1) * sl.n0 + (k - sl.off2) * sl.n0 * sl.n1);
 }
@@ -361,10 +382,9 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
     const float cB = a.irk == 2 ? kB3 : kB2, cA = a.irk == 2 ? 1.0f : kA3rk;
     const uint32_t m_bytes = (need_m ? 9 : 0) * NTHR * G::ES + (need_t ? 9 : 0) * NTHR * G::ES;
     const float rDH = a.rDH, DT = a.DT;
-    // stencil weights with the MacCormack sign and 1/DH folded in
-    const float wx[5] = {FB1 * kAm1 * rDH, FB1 * kA0 * rDH, FB1 * kA1 * rDH, FB1 * kA2 * rDH, FB1 * kA3 * rDH};
-    const float wy[5] = {FB2 * kAm1 * rDH, FB2 * kA0 * rDH, FB2 * kA1 * rDH, FB2 * kA2 * rDH, FB2 * kA3 * rDH};
-    const float wz[5] = {FB3 * kAm1 * rDH, FB3 * kA0 * rDH, FB3 * kA1 * rDH, FB3 * kA2 * rDH, FB3 * kA3 * rDH};
+    // the MacCormack sign and 1/DH of each direction, applied to its elastic
+    // combination (the stencil sums use the bare weights)
+    const float gx = FB1 * rDH, gy = FB2 * rDH, gz = FB3 * rDH;
     const float *px = a.pml, *py = a.pml + 3 * L.nx_, *pz = a.pml + 3 * L.nx_ + 3 * L.ny_;
     const long long fs = L.fs;
     int bxi, byi, kb, ke;
@@ -411,9 +431,9 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         for (int o = 0; o < NM && o < nout; ++o) issue_m(o);
     }
 
-    // per-column PML beta times DT
+    // per-column PML beta times DT, with the direction's sign and 1/DH
     const int ic = valid ? i : HALO, jc = valid ? j : HALO;
-    const float bxd = px[L.nx_ + ic] * DT, byd = py[L.ny_ + jc] * DT;
+    const float bxd = px[L.nx_ + ic] * DT * gx, byd = py[L.ny_ + jc] * DT * gy;
     // PML variant: the x (x1/x2) and y (y1/y2) slab of this column
     int sx = -1, sy = -1;
     if (PMLK && valid && a.nslab) {
@@ -421,9 +441,21 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
       sx = i < HALO + np ? 0 : i >= L.nx_ - HALO - np ? 3 : -1;
       sy = j < HALO + np ? 1 : j >= L.ny_ - HALO - np ? 4 : -1;
     }
+    // PML profile d (times the direction's sign and 1/DH, as it multiplies
+    // the elastic combination), alpha + d and beta of this column
     float dlx = 0.f, btx = 0.f, adx = 0.f, dly = 0.f, bty = 0.f, ady = 0.f;
-    if (PMLK && sx >= 0) { dlx = __ldg(px + 2 * L.nx_ + i); btx = __ldg(px + L.nx_ + i); adx = __ldg(px + i) + dlx; }
-    if (PMLK && sy >= 0) { dly = __ldg(py + 2 * L.ny_ + j); bty = __ldg(py + L.ny_ + j); ady = __ldg(py + j) + dly; }
+    if (PMLK && sx >= 0) {
+      const float d = __ldg(px + 2 * L.nx_ + i);
+      btx = __ldg(px + L.nx_ + i);
+      adx = __ldg(px + i) + d;
+      dlx = d * gx;
+    }
+    if (PMLK && sy >= 0) {
+      const float d = __ldg(py + 2 * L.ny_ + j);
+      bty = __ldg(py + L.ny_ + j);
+      ady = __ldg(py + j) + d;
+      dly = d * gy;
+    }
 
     // z window in registers: physical slot n mod 5 holds input plane q_n; the
     // plane loop is unrolled five times so that every slot index is a
@@ -471,65 +503,118 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         }
         const float mu = ldv(cf + 9 * NTHR + cidx), lam = ldv(cf + 10 * NTHR + cidx);
         const float bu = ldv(cf + 11 * NTHR + cidx) * (float)CRHO_OF<S>::v;
-        const float bzd = __ldg(pz + L.nz_ + k) * DT;
+        const float bzd = __ldg(pz + L.nz_ + k) * DT * gz;
         float h[9], Lr[9], E[9];
+        // Fields are taken in pairs (0,1) (2,3) (4,5) (6,7) and 8 for the
+        // stencil sums, the increment and the RK combination.  The centre
+        // tap of the x and y stencils, plane k at this point, is window slot
+        // P1 (loaded from the same shared-memory plane one iteration ago).
         // x direction
 #pragma unroll
-        for (int v = 0; v < 9; ++v) {
-          const S *row = xy + (v * BY + ys) * BX + xs;
-          Lr[v] = wx[0] * ldv(row - FB1) + wx[1] * ldv(row) + wx[2] * ldv(row + FB1) +
-                  wx[3] * ldv(row + 2 * FB1) + wx[4] * ldv(row + 3 * FB1);
+        for (int v = 0; v < 8; v += 2) {
+          const S *r0 = xy + (v * BY + ys) * BX + xs, *r1 = r0 + BY * BX;
+          const float2 s = stencil2(pk(ldv(r0 - FB1), ldv(r1 - FB1)), pk(win[v][P1], win[v + 1][P1]),
+                                    pk(ldv(r0 + FB1), ldv(r1 + FB1)),
+                                    pk(ldv(r0 + 2 * FB1), ldv(r1 + 2 * FB1)),
+                                    pk(ldv(r0 + 3 * FB1), ldv(r1 + 3 * FB1)));
+          Lr[v] = s.x;
+          Lr[v + 1] = s.y;
+        }
+        {
+          const S *r0 = xy + (8 * BY + ys) * BX + xs;
+          Lr[8] = stencil1(ldv(r0 - FB1), win[8][P1], ldv(r0 + FB1), ldv(r0 + 2 * FB1), ldv(r0 + 3 * FB1));
         }
         elastic9(mx, Lr, mu, lam, bu, E);
 #pragma unroll
-        for (int v = 0; v < 9; ++v) h[v] = bxd * E[v];
+        for (int v = 0; v < 8; v += 2) {
+          const float2 hp = __fmul2_rn(pk(bxd), pk(E[v], E[v + 1]));
+          h[v] = hp.x;
+          h[v + 1] = hp.y;
+        }
+        h[8] = bxd * E[8];
         if (PMLK && sx >= 0) {  // profile values d, alpha + d, beta at this x
           pml_apply<RK, HP>(a.slab[sx], slab_pos(a.slab[sx], i, j, k), E, dlx, adx, btx, DT, cB, cA, h, pin);
         }
         // y direction
 #pragma unroll
-        for (int v = 0; v < 9; ++v) {
-          const S *col = xy + (v * BY + ys) * BX + xs;
-          Lr[v] = wy[0] * ldv(col - FB2 * BX) + wy[1] * ldv(col) + wy[2] * ldv(col + FB2 * BX) +
-                  wy[3] * ldv(col + 2 * FB2 * BX) + wy[4] * ldv(col + 3 * FB2 * BX);
+        for (int v = 0; v < 8; v += 2) {
+          const S *c0 = xy + (v * BY + ys) * BX + xs, *c1 = c0 + BY * BX;
+          const float2 s = stencil2(pk(ldv(c0 - FB2 * BX), ldv(c1 - FB2 * BX)), pk(win[v][P1], win[v + 1][P1]),
+                                    pk(ldv(c0 + FB2 * BX), ldv(c1 + FB2 * BX)),
+                                    pk(ldv(c0 + 2 * FB2 * BX), ldv(c1 + 2 * FB2 * BX)),
+                                    pk(ldv(c0 + 3 * FB2 * BX), ldv(c1 + 3 * FB2 * BX)));
+          Lr[v] = s.x;
+          Lr[v + 1] = s.y;
+        }
+        {
+          const S *c0 = xy + (8 * BY + ys) * BX + xs;
+          Lr[8] = stencil1(ldv(c0 - FB2 * BX), win[8][P1], ldv(c0 + FB2 * BX), ldv(c0 + 2 * FB2 * BX),
+                           ldv(c0 + 3 * FB2 * BX));
         }
         elastic9(my, Lr, mu, lam, bu, E);
 #pragma unroll
-        for (int v = 0; v < 9; ++v) h[v] += byd * E[v];
+        for (int v = 0; v < 8; v += 2) {
+          const float2 hp = __ffma2_rn(pk(byd), pk(E[v], E[v + 1]), pk(h[v], h[v + 1]));
+          h[v] = hp.x;
+          h[v + 1] = hp.y;
+        }
+        h[8] += byd * E[8];
         if (PMLK && sy >= 0) {
           PmlIn late;
           pml_apply<RK, 0>(a.slab[sy], slab_pos(a.slab[sy], i, j, k), E, dly, ady, bty, DT, cB, cA, h, late);
         }
         // z direction: W[k - m*DIR] for m = -1..3 sits in slots P0 (q = k + DIR) .. P4
 #pragma unroll
-        for (int v = 0; v < 9; ++v)
-          Lr[v] = wz[0] * win[v][P0] + wz[1] * win[v][P1] + wz[2] * win[v][P2] +
-                  wz[3] * win[v][P3] + wz[4] * win[v][P4];
+        for (int v = 0; v < 8; v += 2) {
+          const float2 s = stencil2(pk(win[v][P0], win[v + 1][P0]), pk(win[v][P1], win[v + 1][P1]),
+                                    pk(win[v][P2], win[v + 1][P2]), pk(win[v][P3], win[v + 1][P3]),
+                                    pk(win[v][P4], win[v + 1][P4]));
+          Lr[v] = s.x;
+          Lr[v + 1] = s.y;
+        }
+        Lr[8] = stencil1(win[8][P0], win[8][P1], win[8][P2], win[8][P3], win[8][P4]);
         elastic9(mz, Lr, mu, lam, bu, E);
 #pragma unroll
-        for (int v = 0; v < 9; ++v) h[v] += bzd * E[v];
-        if (PMLK && a.nslab && k < HALO + a.npml) {
-          const float dlz = __ldg(pz + 2 * L.nz_ + k), btz = __ldg(pz + L.nz_ + k), adz = __ldg(pz + k) + dlz;
-          PmlIn late;
-          pml_apply<RK, 0>(a.slab[2], slab_pos(a.slab[2], i, j, k), E, dlz, adz, btz, DT, cB, cA, h, late);
+        for (int v = 0; v < 8; v += 2) {
+          const float2 hp = __ffma2_rn(pk(bzd), pk(E[v], E[v + 1]), pk(h[v], h[v + 1]));
+          h[v] = hp.x;
+          h[v + 1] = hp.y;
         }
-        // RK4 combination (wave_rk.cpp:13-99)
+        h[8] += bzd * E[8];
+        if (PMLK && a.nslab && k < HALO + a.npml) {
+          const float d = __ldg(pz + 2 * L.nz_ + k), btz = __ldg(pz + L.nz_ + k), adz = __ldg(pz + k) + d;
+          PmlIn late;
+          pml_apply<RK, 0>(a.slab[2], slab_pos(a.slab[2], i, j, k), E, d * gz, adz, btz, DT, cB, cA, h, late);
+        }
+        // RK4 combination (wave_rk.cpp:13-99), two fields at a time:
+        // stage 0: t = m + B1 h, out = m + A2 h (the stage input at k is the step state m);
+        // stages 1-2: t += B h, out = m + A h; stage 3: out = t + B4 h
         const S *ms = (const S *)(smem + G::OFF_M + ((fm0 + o) % NM) * G::M_BYTES);
         const S *ts = ms + 9 * NTHR;
         const long long ctr = L.at(i, j, k);
+        const float cT = RK == 0 ? kB1 : RK == 1 ? cB : 0.0f;
+        const float cO = RK == 0 ? kA2rk : RK == 1 ? cA : kB4;
 #pragma unroll
-        for (int v = 0; v < 9; ++v) {
-          const float hv = h[v];
+        for (int v = 0; v < 9; v += 2) {
+          const bool two = v < 8;
+          const float2 hv = pk(h[v], two ? h[v + 1] : 0.0f);
           const long long q = ctr + v * fs;
+          float2 base_t, base_o;  // what t and the output add the increment to
           if (RK == 0) {
-            const float m0 = win[v][P1];  // the stage input at k is the step state
-            stv(a.t + q, m0 + kB1 * hv);
-            stv(a.wout + q, m0 + kA2rk * hv);
+            base_t = base_o = pk(win[v][P1], two ? win[v + 1][P1] : 0.0f);
           } else if (RK == 1) {
-            stv(a.t + q, ldv(ts + v * NTHR + cidx) + cB * hv);
-            stv(a.wout + q, ldv(ms + v * NTHR + cidx) + cA * hv);
+            base_t = pk(ldv(ts + v * NTHR + cidx), two ? ldv(ts + (v + 1) * NTHR + cidx) : 0.0f);
+            base_o = pk(ldv(ms + v * NTHR + cidx), two ? ldv(ms + (v + 1) * NTHR + cidx) : 0.0f);
           } else {
-            stv(a.wout + q, ldv(ts + v * NTHR + cidx) + kB4 * hv);
+            base_o = pk(ldv(ts + v * NTHR + cidx), two ? ldv(ts + (v + 1) * NTHR + cidx) : 0.0f);
+          }
+          const float2 wo = __ffma2_rn(pk(cO), hv, base_o);
+          stv(a.wout + q, wo.x);
+          if (two) stv(a.wout + q + fs, wo.y);
+          if (RK <= 1) {
+            const float2 wt = __ffma2_rn(pk(cT), hv, base_t);
+            stv(a.t + q, wt.x);
+            if (two) stv(a.t + q + fs, wt.y);
           }
         }
       }
