@@ -163,41 +163,42 @@ __device__ __forceinline__ unsigned slab_pos(const SlabDev<float> &sl, int i, in
 //
 // A point's inputs are the auxiliary input (part 1), what the stage adds the
 // increment to (part 2: m in stages 1-2, t in stage 3) and t (part 4, stages
-// 1-2).  pml_load<RK, H> loads the parts in H for all nine fields, so that
+// 1-2).  pml_load<RK> loads the parts in a mask for all nine fields, so that
 // the loads can be issued at the top of a plane iteration and their latency
-// overlaps the stencil work; pml_apply<RK, H> loads the other parts (three
-// fields at a time, each group's loads before its stores) and updates.
+// overlaps the stencil work; pml_apply<RK> is told which parts are already
+// in registers (a compile-time or a per-thread mask), loads the others
+// (three fields at a time, each group's loads before its stores) and updates.
 template <int RK> constexpr int pml_parts() { return RK == 0 ? 1 : RK == 3 ? 3 : 7; }
 struct PmlIn {
   float a[9], b[9], t[9];
 };
-template <int RK, int H>
+template <int RK>
 __device__ __forceinline__ void pml_load_fields(const SlabDev<float> &sl, unsigned pos, int v0,
-                                                int nv, PmlIn &in) {
-  constexpr int P = pml_parts<RK>() & H;
+                                                int nv, int mask, PmlIn &in) {
+  constexpr int P = pml_parts<RK>();
   const unsigned np = (unsigned)sl.np;
 #pragma unroll
   for (int v = v0; v < v0 + nv; ++v) {
     const unsigned q = v * np + pos;
-    if (P & 1) in.a[v] = sl.ain[q];
-    if (P & 2) in.b[v] = RK == 3 ? sl.at[q] : sl.am[q];
-    if (P & 4) in.t[v] = sl.at[q];
+    if ((P & 1) && (mask & 1)) in.a[v] = sl.ain[q];
+    if ((P & 2) && (mask & 2)) in.b[v] = RK == 3 ? sl.at[q] : sl.am[q];
+    if ((P & 4) && (mask & 4)) in.t[v] = sl.at[q];
   }
 }
-template <int RK, int H>
-__device__ __forceinline__ void pml_load(const SlabDev<float> &sl, unsigned pos, PmlIn &in) {
-  pml_load_fields<RK, H>(sl, pos, 0, 9, in);
+template <int RK>
+__device__ __forceinline__ void pml_load(const SlabDev<float> &sl, unsigned pos, int mask, PmlIn &in) {
+  pml_load_fields<RK>(sl, pos, 0, 9, mask, in);
 }
-template <int RK, int H>
+template <int RK>
 __device__ __forceinline__ void pml_apply(const SlabDev<float> &sl, unsigned pos, const float E[9],
                                           float dl, float ad, float bt, float DT, float cB,
-                                          float cA, float h[9], PmlIn &in) {
+                                          float cA, float h[9], int held, PmlIn &in) {
   const unsigned np = (unsigned)sl.np;
   float *__restrict__ aout = sl.aout;
   float *__restrict__ at = sl.at;
 #pragma unroll
   for (int g = 0; g < 9; g += 3) {
-    pml_load_fields<RK, 7 & ~H>(sl, pos, g, 3, in);
+    pml_load_fields<RK>(sl, pos, g, 3, 7 & ~held, in);
 #pragma unroll
     for (int v = g; v < g + 3; ++v) {
       const unsigned q = v * np + pos;
@@ -216,9 +217,11 @@ __device__ __forceinline__ void pml_apply(const SlabDev<float> &sl, unsigned pos
     }
   }
 }
-// The parts of an x-slab point loaded at the top of its plane iteration:
-// all of them in stages 0 and 3; the auxiliary input alone in stages 1-2,
-// where holding all three parts (27 registers) across the stencils spills.
+// The parts of a slab point loaded at the top of its plane iteration: all of
+// them in stages 0 and 3; the auxiliary input alone in stages 1-2, where
+// holding all three parts (27 registers) across the stencils spills.  The
+// loads are for the point's first slab in application order (x, then y,
+// then the bottom z slab); a corner point loads its later slabs in place.
 template <int RK> constexpr int hoist_parts() { return RK == 1 ? 1 : pml_parts<RK>(); }
 
 struct Maps {
@@ -346,7 +349,10 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
   constexpr int NW = G::NW, NC = G::NC, NM = G::NM, BX = G::BX;
   constexpr int DIR = -FB3;  // sweep direction in z
   extern __shared__ unsigned char smem_raw[];
-  unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  // 128-byte aligned base, derived by pointer arithmetic on the shared array
+  // (not through an integer) so that every access through it compiles to a
+  // shared-memory load with a 32-bit address
+  unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   uint64_t *bw = (uint64_t *)(smem + G::OFF_BAR);
   uint64_t *bc = bw + NW;
   uint64_t *bm = bc + NC;
@@ -472,10 +478,15 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
       constexpr int P0 = R, P1 = (R + 4) % 5, P2 = (R + 3) % 5, P3 = (R + 2) % 5, P4 = (R + 1) % 5;
       const int o = n - 4;  // output index of this iteration (o < 0: window warm-up)
       constexpr int HP = hoist_parts<RK>();
-      // the x-slab inputs of this plane's point, issued before the waits
+      // the inputs of this plane's point in its first slab (x, y or the
+      // bottom z slab), issued before the waits
       PmlIn pin;
       const int kk = q0 + n * DIR - DIR;
-      if (PMLK && o >= 0 && sx >= 0) pml_load<RK, HP>(a.slab[sx], slab_pos(a.slab[sx], i, j, kk), pin);
+      int sh = -1;  // the slab whose parts HP are in pin
+      if (PMLK && o >= 0 && valid && a.nslab) {
+        sh = sx >= 0 ? sx : sy >= 0 ? sy : kk < HALO + a.npml ? 2 : -1;
+        if (sh >= 0) pml_load<RK>(a.slab[sh], slab_pos(a.slab[sh], i, j, kk), HP, pin);
+      }
       bool ok = mbar_wait_bounded(smem_u32(&bw[(fw0 + n) % NW]), ((fw0 + n) / NW) & 1);
       if (o >= 0) {
         ok = ok && mbar_wait_bounded(smem_u32(&bc[(fc0 + o) % NC]), ((fc0 + o) / NC) & 1);
@@ -533,7 +544,7 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         }
         h[8] = bxd * E[8];
         if (PMLK && sx >= 0) {  // profile values d, alpha + d, beta at this x
-          pml_apply<RK, HP>(a.slab[sx], slab_pos(a.slab[sx], i, j, k), E, dlx, adx, btx, DT, cB, cA, h, pin);
+          pml_apply<RK>(a.slab[sx], slab_pos(a.slab[sx], i, j, k), E, dlx, adx, btx, DT, cB, cA, h, HP, pin);
         }
         // y direction
 #pragma unroll
@@ -560,8 +571,8 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         }
         h[8] += byd * E[8];
         if (PMLK && sy >= 0) {
-          PmlIn late;
-          pml_apply<RK, 0>(a.slab[sy], slab_pos(a.slab[sy], i, j, k), E, dly, ady, bty, DT, cB, cA, h, late);
+          pml_apply<RK>(a.slab[sy], slab_pos(a.slab[sy], i, j, k), E, dly, ady, bty, DT, cB, cA, h,
+                        sh == sy ? HP : 0, pin);
         }
         // z direction: W[k - m*DIR] for m = -1..3 sits in slots P0 (q = k + DIR) .. P4
 #pragma unroll
@@ -583,8 +594,8 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         h[8] += bzd * E[8];
         if (PMLK && a.nslab && k < HALO + a.npml) {
           const float d = __ldg(pz + 2 * L.nz_ + k), btz = __ldg(pz + L.nz_ + k), adz = __ldg(pz + k) + d;
-          PmlIn late;
-          pml_apply<RK, 0>(a.slab[2], slab_pos(a.slab[2], i, j, k), E, d * gz, adz, btz, DT, cB, cA, h, late);
+          pml_apply<RK>(a.slab[2], slab_pos(a.slab[2], i, j, k), E, d * gz, adz, btz, DT, cB, cA, h,
+                        sh == 2 ? HP : 0, pin);
         }
         // RK4 combination (wave_rk.cpp:13-99), two fields at a time:
         // stage 0: t = m + B1 h, out = m + A2 h (the stage input at k is the step state m);
