@@ -66,11 +66,17 @@ __device__ __forceinline__ void jt_rows(const S *W, const S *cjm, long long num,
   r[2] = (m0 * (R)ldv(W + q + num * 7) + m1 * (R)ldv(W + q + num * 8) + m2 * (R)ldv(W + q + num * 5)) * J;
 }
 
-template <typename R> __device__ __forceinline__ R LJT(const R *jt, int fb, R rDH) {
-  return (R)fb *
-         ((R)kAm1 * jt[3 - fb] + (R)kA0 * jt[3] + (R)kA1 * jt[3 + fb] + (R)kA2 * jt[3 + 2 * fb] +
-          (R)kA3 * jt[3 + 3 * fb]) *
+// The sign FB is dispatched to a template so that every index into the row
+// array is a compile-time constant (the array stays in registers); the
+// expression and its operation order are the same for both signs.
+template <int FB, typename R> __device__ __forceinline__ R LJT_fb(const R *jt, R rDH) {
+  return (R)FB *
+         ((R)kAm1 * jt[3 - FB] + (R)kA0 * jt[3] + (R)kA1 * jt[3 + FB] + (R)kA2 * jt[3 + 2 * FB] +
+          (R)kA3 * jt[3 + 3 * FB]) *
          rDH;
+}
+template <typename R> __device__ __forceinline__ R LJT(const R *jt, int fb, R rDH) {
+  return fb > 0 ? LJT_fb<1>(jt, rDH) : LJT_fb<-1>(jt, rDH);
 }
 
 template <typename S>
@@ -125,13 +131,20 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
       jt_rows(W, cjm, num, c + (l - HALO) * sy, 1, r);
       jy[0][l] = r[0]; jy[1][l] = r[1]; jy[2][l] = r[2];
     }
-    for (int l = 0; l < ks; ++l) {
-      jt_rows(W, cjm, num, c + (l - HALO) * sz, 2, r);
-      jz[0][l] = r[0]; jz[1][l] = r[1]; jz[2][l] = r[2];
+    // rows below the surface; zero at it; above it the antisymmetric image
+    // -row(2 ks - l), recomputed at the mirrored point (the same bits)
+#pragma unroll
+    for (int l = 0; l < 7; ++l) {
+      if (l < ks) {
+        jt_rows(W, cjm, num, c + (l - HALO) * sz, 2, r);
+        jz[0][l] = r[0]; jz[1][l] = r[1]; jz[2][l] = r[2];
+      } else if (l == ks) {
+        jz[0][l] = jz[1][l] = jz[2][l] = (R)0.0f;
+      } else {
+        jt_rows(W, cjm, num, c + (2 * ks - l - HALO) * sz, 2, r);
+        jz[0][l] = -r[0]; jz[1][l] = -r[1]; jz[2][l] = -r[2];
+      }
     }
-    jz[0][ks] = jz[1][ks] = jz[2][ks] = (R)0.0f;
-    for (int l = ks + 1; l < 7; ++l)
-      for (int q = 0; q < 3; ++q) jz[q][l] = -jz[q][2 * ks - l];
     const R Jinv = (R)1.0f / (R)ldv(cjm + c + num * 9);
 #pragma unroll
     for (int q = 0; q < 3; ++q)
@@ -185,6 +198,8 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
     const int i0 = i - sl.off0, j0 = j - sl.off1, k0 = k - sl.off2;
     if (i0 < 0 || i0 >= sl.n0 || j0 < 0 || j0 >= sl.n1 || k0 < 0 || k0 >= sl.n2) continue;
     const int ax = sl.axis;
+    const long long sa = ax == 0 ? sx : ax == 1 ? sy : sz;  // the slab's stride and sign
+    const int fa = ax == 0 ? a.fb1 : ax == 1 ? a.fb2 : a.fb3;
     const int l = ax == 0 ? i : ax == 1 ? j : k;
     const R *prof = ax == 0 ? px : ax == 1 ? py : pz;
     const int nax = ax == 0 ? nx_ : ax == 1 ? ny_ : nz_;
@@ -196,9 +211,9 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
     R m[3], dv[3], dt[6], term[9], ha[9];
     metric(cjm, num, c, ax, m);
 #pragma unroll
-    for (int v = 0; v < 3; ++v) dv[v] = Lop(W + v * num, c, stv3[ax], fbv[ax], rDH) * dl;
+    for (int v = 0; v < 3; ++v) dv[v] = Lop(W + v * num, c, sa, fa, rDH) * dl;
 #pragma unroll
-    for (int v = 0; v < 6; ++v) dt[v] = Lop(W + (3 + v) * num, c, stv3[ax], fbv[ax], rDH) * dl;
+    for (int v = 0; v < 6; ++v) dt[v] = Lop(W + (3 + v) * num, c, sa, fa, rDH) * dl;
     elastic(m, dv, dt, mu, lam, b * (R)CRHO_OF<S>::v, term);
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
@@ -213,7 +228,7 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
       R vd[3], vz[3], zt[3], t[9];
       const R z6[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
-      for (int v = 0; v < 3; ++v) vd[v] = Lop(W + v * num, c, stv3[ax], fbv[ax], rDH) * dl;
+      for (int v = 0; v < 3; ++v) vd[v] = Lop(W + v * num, c, sa, fa, rDH) * dl;
 #pragma unroll
       for (int q = 0; q < 3; ++q) vz[q] = M[3 * q] * vd[0] + M[3 * q + 1] * vd[1] + M[3 * q + 2] * vd[2];
       metric(cjm, num, c, 2, zt);
