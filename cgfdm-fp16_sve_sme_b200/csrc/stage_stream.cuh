@@ -24,11 +24,12 @@
 // wavefield and auxiliaries are fused: each field is read and written once
 // per stage, stores are whole 128-byte lines per warp row.
 //
-// Arithmetic: FP32 with FMA contraction; the sign FB and 1/DH are folded into
-// the stencil weights and each direction's elastic combination is formed once
-// and scaled by the PML beta (main update) and d (auxiliary update), equal to
-// the reference up to rounding.  The three free-surface layers are left to
-// the exact-order kernel.
+// Arithmetic: FP32 with FMA contraction, two fields per packed FP32x2
+// instruction in the stencil sums, increments and RK update; the stencil
+// sums use the bare MacCormack weights, and each direction's elastic
+// combination is formed once and scaled by the sign FB, 1/DH and the PML beta
+// (main update) or d (auxiliary update), equal to the reference up to
+// rounding.  The three free-surface layers are left to the exact-order kernel.
 //
 // Every mbarrier wait is bounded (2^31 clock cycles); on expiry the CTA sets
 // the error flag, drains the copies it issued (again bounded) and returns.
@@ -188,6 +189,20 @@ __device__ __forceinline__ void pml_load_fields(const SlabDev<float> &sl, unsign
 template <int RK>
 __device__ __forceinline__ void pml_load(const SlabDev<float> &sl, unsigned pos, int mask, PmlIn &in) {
   pml_load_fields<RK>(sl, pos, 0, 9, mask, in);
+}
+// L1 prefetch of the parts in a mask (no registers held), for the parts the
+// stage needs but does not keep in registers across the stencils.
+template <int RK>
+__device__ __forceinline__ void pml_prefetch(const SlabDev<float> &sl, unsigned pos, int mask) {
+  constexpr int P = pml_parts<RK>();
+  const unsigned np = (unsigned)sl.np;
+#pragma unroll
+  for (int v = 0; v < 9; ++v) {
+    const unsigned q = v * np + pos;
+    if ((P & 2) && (mask & 2))
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(RK == 3 ? sl.at + q : sl.am + q));
+    if ((P & 4) && (mask & 4)) asm volatile("prefetch.global.L1 [%0];" ::"l"(sl.at + q));
+  }
 }
 template <int RK>
 __device__ __forceinline__ void pml_apply(const SlabDev<float> &sl, unsigned pos, const float E[9],
@@ -485,7 +500,11 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
       int sh = -1;  // the slab whose parts HP are in pin
       if (PMLK && o >= 0 && valid && a.nslab) {
         sh = sx >= 0 ? sx : sy >= 0 ? sy : kk < HALO + a.npml ? 2 : -1;
-        if (sh >= 0) pml_load<RK>(a.slab[sh], slab_pos(a.slab[sh], i, j, kk), HP, pin);
+        if (sh >= 0) {
+          const unsigned pos = slab_pos(a.slab[sh], i, j, kk);
+          pml_load<RK>(a.slab[sh], pos, HP, pin);
+          if (HP != pml_parts<RK>()) pml_prefetch<RK>(a.slab[sh], pos, pml_parts<RK>() & ~HP);
+        }
       }
       bool ok = mbar_wait_bounded(smem_u32(&bw[(fw0 + n) % NW]), ((fw0 + n) / NW) & 1);
       if (o >= 0) {
