@@ -131,6 +131,44 @@ __device__ __forceinline__ void elastic9(const float m[3], const float L[9], flo
   E[8] = (m[2] * L[1] + m[1] * L[2]) * mu;
 }
 
+// The interior variant's form of the three directions' elastic combinations
+// and their sum into the stage increment (wave_deriv.cpp:163-201,
+// reassociated; equal up to rounding): mu, lambda and the buoyancy are the
+// point's own, so each direction adds its metric row scaled by the
+// direction factor g times the derivatives, and mu, lambda and b multiply
+// the sums once (the PML variant keeps the per-direction combination E,
+// which its auxiliary update needs).
+struct ElasticSum {
+  float v0, v1, v2;  // velocity rows, before b
+  float nx, ny, nz;  // normal terms m_x dVx, m_y dVy, m_z dVz
+  float s6, s7, s8;  // shear terms, before mu
+  template <bool FIRST>
+  __device__ __forceinline__ void add(const float m[3], float g, const float L[9]) {
+    const float a0 = g * m[0], a1 = g * m[1], a2 = g * m[2];
+    v0 = fmaf(a2, L[7], fmaf(a1, L[6], FIRST ? a0 * L[3] : fmaf(a0, L[3], v0)));
+    v1 = fmaf(a2, L[8], fmaf(a1, L[4], FIRST ? a0 * L[6] : fmaf(a0, L[6], v1)));
+    v2 = fmaf(a2, L[5], fmaf(a1, L[8], FIRST ? a0 * L[7] : fmaf(a0, L[7], v2)));
+    nx = FIRST ? a0 * L[0] : fmaf(a0, L[0], nx);
+    ny = FIRST ? a1 * L[1] : fmaf(a1, L[1], ny);
+    nz = FIRST ? a2 * L[2] : fmaf(a2, L[2], nz);
+    s6 = fmaf(a0, L[1], FIRST ? a1 * L[0] : fmaf(a1, L[0], s6));
+    s7 = fmaf(a0, L[2], FIRST ? a2 * L[0] : fmaf(a2, L[0], s7));
+    s8 = fmaf(a1, L[2], FIRST ? a2 * L[1] : fmaf(a2, L[1], s8));
+  }
+  __device__ __forceinline__ void finish(float mu, float lam, float b, float h[9]) const {
+    h[0] = v0 * b;
+    h[1] = v1 * b;
+    h[2] = v2 * b;
+    const float div = (nx + ny + nz) * lam, tmu = 2.0f * mu;
+    h[3] = fmaf(tmu, nx, div);
+    h[4] = fmaf(tmu, ny, div);
+    h[5] = fmaf(tmu, nz, div);
+    h[6] = s6 * mu;
+    h[7] = s7 * mu;
+    h[8] = s8 * mu;
+  }
+};
+
 // Packed FP32x2 arithmetic (FFMA2 / FMUL2 on sm_100): one instruction applies
 // the same operation to two fields of a point, each lane rounding exactly as
 // the scalar operation would.
@@ -535,6 +573,7 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         const float bu = ldv(cf + 11 * NTHR + cidx) * (float)CRHO_OF<S>::v;
         const float bzd = __ldg(pz + L.nz_ + k) * DT * gz;
         float h[9], Lr[9], E[9];
+        ElasticSum es;
         // Fields are taken in pairs (0,1) (2,3) (4,5) (6,7) and 8 for the
         // stencil sums, the increment and the RK combination.  The centre
         // tap of the x and y stencils, plane k at this point, is window slot
@@ -554,16 +593,20 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
           const S *r0 = xy + (8 * BY + ys) * BX + xs;
           Lr[8] = stencil1(ldv(r0 - FB1), win[8][P1], ldv(r0 + FB1), ldv(r0 + 2 * FB1), ldv(r0 + 3 * FB1));
         }
-        elastic9(mx, Lr, mu, lam, bu, E);
+        if constexpr (PMLK) {
+          elastic9(mx, Lr, mu, lam, bu, E);
 #pragma unroll
-        for (int v = 0; v < 8; v += 2) {
-          const float2 hp = __fmul2_rn(pk(bxd), pk(E[v], E[v + 1]));
-          h[v] = hp.x;
-          h[v + 1] = hp.y;
-        }
-        h[8] = bxd * E[8];
-        if (PMLK && sx >= 0) {  // profile values d, alpha + d, beta at this x
-          pml_apply<RK>(a.slab[sx], slab_pos(a.slab[sx], i, j, k), E, dlx, adx, btx, DT, cB, cA, h, HP, pin);
+          for (int v = 0; v < 8; v += 2) {
+            const float2 hp = __fmul2_rn(pk(bxd), pk(E[v], E[v + 1]));
+            h[v] = hp.x;
+            h[v + 1] = hp.y;
+          }
+          h[8] = bxd * E[8];
+          if (sx >= 0) {  // profile values d, alpha + d, beta at this x
+            pml_apply<RK>(a.slab[sx], slab_pos(a.slab[sx], i, j, k), E, dlx, adx, btx, DT, cB, cA, h, HP, pin);
+          }
+        } else {
+          es.add<true>(mx, bxd, Lr);
         }
         // y direction
 #pragma unroll
@@ -581,17 +624,21 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
           Lr[8] = stencil1(ldv(c0 - FB2 * BX), win[8][P1], ldv(c0 + FB2 * BX), ldv(c0 + 2 * FB2 * BX),
                            ldv(c0 + 3 * FB2 * BX));
         }
-        elastic9(my, Lr, mu, lam, bu, E);
+        if constexpr (PMLK) {
+          elastic9(my, Lr, mu, lam, bu, E);
 #pragma unroll
-        for (int v = 0; v < 8; v += 2) {
-          const float2 hp = __ffma2_rn(pk(byd), pk(E[v], E[v + 1]), pk(h[v], h[v + 1]));
-          h[v] = hp.x;
-          h[v + 1] = hp.y;
-        }
-        h[8] += byd * E[8];
-        if (PMLK && sy >= 0) {
-          pml_apply<RK>(a.slab[sy], slab_pos(a.slab[sy], i, j, k), E, dly, ady, bty, DT, cB, cA, h,
-                        sh == sy ? HP : 0, pin);
+          for (int v = 0; v < 8; v += 2) {
+            const float2 hp = __ffma2_rn(pk(byd), pk(E[v], E[v + 1]), pk(h[v], h[v + 1]));
+            h[v] = hp.x;
+            h[v + 1] = hp.y;
+          }
+          h[8] += byd * E[8];
+          if (sy >= 0) {
+            pml_apply<RK>(a.slab[sy], slab_pos(a.slab[sy], i, j, k), E, dly, ady, bty, DT, cB, cA, h,
+                          sh == sy ? HP : 0, pin);
+          }
+        } else {
+          es.add<false>(my, byd, Lr);
         }
         // z direction: W[k - m*DIR] for m = -1..3 sits in slots P0 (q = k + DIR) .. P4
 #pragma unroll
@@ -603,18 +650,23 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
           Lr[v + 1] = s.y;
         }
         Lr[8] = stencil1(win[8][P0], win[8][P1], win[8][P2], win[8][P3], win[8][P4]);
-        elastic9(mz, Lr, mu, lam, bu, E);
+        if constexpr (PMLK) {
+          elastic9(mz, Lr, mu, lam, bu, E);
 #pragma unroll
-        for (int v = 0; v < 8; v += 2) {
-          const float2 hp = __ffma2_rn(pk(bzd), pk(E[v], E[v + 1]), pk(h[v], h[v + 1]));
-          h[v] = hp.x;
-          h[v + 1] = hp.y;
-        }
-        h[8] += bzd * E[8];
-        if (PMLK && a.nslab && k < HALO + a.npml) {
-          const float d = __ldg(pz + 2 * L.nz_ + k), btz = __ldg(pz + L.nz_ + k), adz = __ldg(pz + k) + d;
-          pml_apply<RK>(a.slab[2], slab_pos(a.slab[2], i, j, k), E, d * gz, adz, btz, DT, cB, cA, h,
-                        sh == 2 ? HP : 0, pin);
+          for (int v = 0; v < 8; v += 2) {
+            const float2 hp = __ffma2_rn(pk(bzd), pk(E[v], E[v + 1]), pk(h[v], h[v + 1]));
+            h[v] = hp.x;
+            h[v + 1] = hp.y;
+          }
+          h[8] += bzd * E[8];
+          if (a.nslab && k < HALO + a.npml) {
+            const float d = __ldg(pz + 2 * L.nz_ + k), btz = __ldg(pz + L.nz_ + k), adz = __ldg(pz + k) + d;
+            pml_apply<RK>(a.slab[2], slab_pos(a.slab[2], i, j, k), E, d * gz, adz, btz, DT, cB, cA, h,
+                          sh == 2 ? HP : 0, pin);
+          }
+        } else {
+          es.add<false>(mz, bzd, Lr);
+          es.finish(mu, lam, bu, h);
         }
         // RK4 combination (wave_rk.cpp:13-99), two fields at a time:
         // stage 0: t = m + B1 h, out = m + A2 h (the stage input at k is the step state m);
