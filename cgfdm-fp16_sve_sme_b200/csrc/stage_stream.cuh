@@ -16,6 +16,9 @@
 //   C ring (2): the 9 metrics and (mu, lambda, buoyancy) of one output plane;
 //   M ring (2): the RK step state m and accumulator t of one output plane
 //               (stages that read them).
+// With 16-bit storage the interior variant converts each W plane to FP32 once
+// in shared memory (two plane buffers), so its stencils read FP32 like the
+// FP32 kernel instead of converting every tap.
 // Every operand of the stage therefore arrives asynchronously ahead of use;
 // only the PML auxiliaries (a minority of points) are read with plain loads,
 // by a second instantiation (PMLK) that runs the tiles and bottom chunks
@@ -56,7 +59,7 @@ constexpr long long kWaitCycles = 1LL << 31;
 // Tile and shared-memory geometry for storage type S and tile height TYv
 // (16: one 512-thread CTA per SM; 8: 256-thread CTAs, two per SM when their
 // shared memory fits, so one CTA's per-plane barrier overlaps the other's work).
-template <typename S, int TYv> struct Geo {
+template <typename S, int TYv, bool PMLK = false> struct Geo {
   static constexpr int TY = TYv, NTHR = TX * TYv;
   static constexpr int BY = TYv + 4;  // y box: 1 or 3 rows before the tile, 3 or 1 after
   static constexpr int MINB = TYv == 8 ? 2 : 1;
@@ -66,15 +69,37 @@ template <typename S, int TYv> struct Geo {
   static constexpr int W_BYTES = ((9 * BY * BX * ES) + 127) / 128 * 128;
   static constexpr int C_BYTES = 12 * NTHR * ES;                 // 9 metrics + mu, lambda, b
   static constexpr int M_BYTES = 18 * NTHR * ES;                 // m (9) and t (9)
-  static constexpr int NW = ES == 4 ? 3 : 4;
-  static constexpr int NC = ES == 4 ? 2 : 3;
-  static constexpr int NM = ES == 4 ? 2 : 3;
+  // 16-bit storage, interior variant: each W plane is converted to FP32 once,
+  // into one of two plane buffers (by plane parity) that the x and y stencils
+  // read.  The PML variant (latency-bound) reads the 16-bit planes directly
+  // and keeps deeper rings instead.
+  static constexpr bool CONV = ES != 4 && !PMLK;
+  static constexpr int NW = ES == 4 || CONV ? 3 : 4;
+  static constexpr int NC = ES == 4 || CONV ? 2 : 3;
+  static constexpr int NM = NC;
+  static constexpr int F_BYTES = CONV ? ((9 * BY * BX * 4) + 127) / 128 * 128 : 0;
   static constexpr int OFF_C = NW * W_BYTES;
   static constexpr int OFF_M = OFF_C + NC * C_BYTES;
-  static constexpr int OFF_BAR = OFF_M + NM * M_BYTES;
+  static constexpr int OFF_F = OFF_M + NM * M_BYTES;
+  static constexpr int OFF_BAR = OFF_F + 2 * F_BYTES;
   static constexpr int SMEM = OFF_BAR + 8 * (NW + NC + NM) + 128;
   static_assert(SMEM <= 232448, "shared memory budget");
+  static_assert(MINB == 1 || MINB * (SMEM + 1024) <= 233472, "two CTAs per SM");
 };
+
+// Four 16-bit values at p (8-byte aligned) as four floats.
+__device__ __forceinline__ float4 cvt4(const __half *p) {
+  const uint2 r = *(const uint2 *)p;
+  const float2 a = __half22float2(*(const __half2 *)&r.x), b = __half22float2(*(const __half2 *)&r.y);
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 cvt4(const __nv_bfloat16 *p) {
+  const uint2 r = *(const uint2 *)p;
+  const float2 a = __bfloat1622float2(*(const __nv_bfloat162 *)&r.x),
+               b = __bfloat1622float2(*(const __nv_bfloat162 *)&r.y);
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 cvt4(const float *p) { return *(const float4 *)p; }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -397,7 +422,7 @@ template <typename S> struct BatchSrc {
 
 template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK, int RK, typename Src>
 __device__ __forceinline__ void stream_body(const Src &src, int *err) {
-  using G = Geo<S, TYv>;
+  using G = Geo<S, TYv, PMLK>;
   constexpr int TY = G::TY, NTHR = G::NTHR, BY = G::BY;
   constexpr int NW = G::NW, NC = G::NC, NM = G::NM, BX = G::BX;
   constexpr int DIR = -FB3;  // sweep direction in z
@@ -556,11 +581,23 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
       __syncthreads();
       if (s_bad) return false;
       const S *tq = (const S *)(smem + ((fw0 + n) % NW) * G::W_BYTES);
+      if constexpr (G::CONV) {  // plane n to FP32 for the stencils of the next iteration
+        constexpr int NE = 9 * BY * BX;
+        static_assert(NE % 4 == 0, "conversion in groups of four");
+        float *fd = (float *)(smem + G::OFF_F + (n & 1) * G::F_BYTES);
+        for (int e = 4 * tid; e < NE; e += 4 * NTHR) *(float4 *)(fd + e) = cvt4(tq + e);
+      }
 #pragma unroll
       for (int v = 0; v < 9; ++v) win[v][P0] = ldv(tq + (v * BY + ys) * BX + xs);
       if (o >= 0 && valid) {
         const int k = q0 + n * DIR - DIR;
-        const S *xy = (const S *)(smem + ((fw0 + n + NW - 1) % NW) * G::W_BYTES);  // plane k
+        // plane k: its FP32 copy, or the W slot itself
+        using XT = std::conditional_t<G::CONV, float, S>;
+        const XT *xy;
+        if constexpr (G::CONV)
+          xy = (const float *)(smem + G::OFF_F + ((n - 1) & 1) * G::F_BYTES);
+        else
+          xy = (const S *)(smem + ((fw0 + n + NW - 1) % NW) * G::W_BYTES);
         const S *cf = (const S *)(smem + G::OFF_C + ((fc0 + o) % NC) * G::C_BYTES);
         float mx[3], my[3], mz[3];
 #pragma unroll
@@ -581,7 +618,7 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         // x direction
 #pragma unroll
         for (int v = 0; v < 8; v += 2) {
-          const S *r0 = xy + (v * BY + ys) * BX + xs, *r1 = r0 + BY * BX;
+          const XT *r0 = xy + (v * BY + ys) * BX + xs, *r1 = r0 + BY * BX;
           const float2 s = stencil2(pk(ldv(r0 - FB1), ldv(r1 - FB1)), pk(win[v][P1], win[v + 1][P1]),
                                     pk(ldv(r0 + FB1), ldv(r1 + FB1)),
                                     pk(ldv(r0 + 2 * FB1), ldv(r1 + 2 * FB1)),
@@ -590,7 +627,7 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
           Lr[v + 1] = s.y;
         }
         {
-          const S *r0 = xy + (8 * BY + ys) * BX + xs;
+          const XT *r0 = xy + (8 * BY + ys) * BX + xs;
           Lr[8] = stencil1(ldv(r0 - FB1), win[8][P1], ldv(r0 + FB1), ldv(r0 + 2 * FB1), ldv(r0 + 3 * FB1));
         }
         if constexpr (PMLK) {
@@ -611,7 +648,7 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         // y direction
 #pragma unroll
         for (int v = 0; v < 8; v += 2) {
-          const S *c0 = xy + (v * BY + ys) * BX + xs, *c1 = c0 + BY * BX;
+          const XT *c0 = xy + (v * BY + ys) * BX + xs, *c1 = c0 + BY * BX;
           const float2 s = stencil2(pk(ldv(c0 - FB2 * BX), ldv(c1 - FB2 * BX)), pk(win[v][P1], win[v + 1][P1]),
                                     pk(ldv(c0 + FB2 * BX), ldv(c1 + FB2 * BX)),
                                     pk(ldv(c0 + 2 * FB2 * BX), ldv(c1 + 2 * FB2 * BX)),
@@ -620,7 +657,7 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
           Lr[v + 1] = s.y;
         }
         {
-          const S *c0 = xy + (8 * BY + ys) * BX + xs;
+          const XT *c0 = xy + (8 * BY + ys) * BX + xs;
           Lr[8] = stencil1(ldv(c0 - FB2 * BX), win[8][P1], ldv(c0 + FB2 * BX), ldv(c0 + 2 * FB2 * BX),
                            ldv(c0 + 3 * FB2 * BX));
         }
@@ -772,7 +809,7 @@ __global__ void __launch_bounds__(TX * 16, 1)
 template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK, int RK>
 cudaError_t launch_variant(const StageArgs<S> &a, const Maps &maps, const Work &wk, int *err,
                            int nsm, cudaStream_t st) {
-  using G = Geo<S, TYv>;
+  using G = Geo<S, TYv, PMLK>;
   static int attr_dev = -1;
   auto kern = stage_stream_kernel<S, TYv, FB1, FB2, FB3, PMLK, RK>;
   const int smem = G::SMEM;
@@ -870,7 +907,7 @@ cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *c
 template <typename S, int FB1, int FB2, int FB3, bool PMLK, int RK>
 cudaError_t launch_batch_variant(const BatchParams<S> &p, int items, int *err, int nsm,
                                  cudaStream_t st) {
-  using G = Geo<S, 16>;
+  using G = Geo<S, 16, PMLK>;
   static_assert(sizeof(BatchParams<S>) <= 32000, "kernel parameter space");
   static int attr_dev = -1;
   auto kern = stage_stream_batch_kernel<S, FB1, FB2, FB3, PMLK, RK>;
