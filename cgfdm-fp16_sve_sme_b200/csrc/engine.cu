@@ -158,7 +158,9 @@ template <typename S> class EngineT : public Engine {
 
   int set_model(const float *cjm, const float *rdz) override {
     CUDA_TRY(cudaSetDevice(d_.device));
-    CUDA_TRY(upload_repacked(cjm, cjm_, 13));
+    int rc = synchronize();  // no stage of this handle may be reading the coefficients
+    if (rc) return rc;
+    CUDA_TRY(upload_through_accumulator(cjm, cjm_, 13));
     std::vector<R> r(rdz, rdz + 18 * g_.nsurf);
     CUDA_TRY(h2d(rdz_, r.data(), sizeof(R) * r.size()));
     host_cjm_J_.assign(cjm + 9 * g_.num, cjm + 10 * g_.num);
@@ -877,6 +879,28 @@ template <typename S> class EngineT : public Engine {
     if (e == cudaSuccess) e = launch_repack_in<S>(tmp, dst, g_.L, nfield, own_stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(own_stream_);
     cudaFree(tmp);
+    return e;
+  }
+
+  // The coefficient upload stages the host fields through the RK accumulator
+  // T, a few fields at a time, instead of allocating a staging buffer as
+  // large as the model: outside a stage T is free (every stage 0 rewrites it
+  // before anything reads it).  T is cleared afterwards.
+  cudaError_t upload_through_accumulator(const float *src, S *dst, int nfield) {
+    const size_t tbytes = sizeof(S) * 9 * (size_t)g_.L.fs;
+    const int per = (int)std::min<size_t>((size_t)nfield, tbytes / (sizeof(float) * (size_t)g_.num));
+    if (per < 1) return upload_repacked(src, dst, nfield);
+    float *stage = (float *)T_;
+    cudaError_t e = cudaSuccess;
+    for (int f0 = 0; f0 < nfield && e == cudaSuccess; f0 += per) {
+      const int nf = std::min(per, nfield - f0);
+      e = cudaMemcpyAsync(stage, src + (size_t)f0 * g_.num, sizeof(float) * nf * (size_t)g_.num,
+                          cudaMemcpyHostToDevice, own_stream_);
+      if (e == cudaSuccess)
+        e = launch_repack_in<S>(stage, dst + (size_t)f0 * g_.L.fs, g_.L, nf, own_stream_);
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(T_, 0, tbytes, own_stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(own_stream_);
     return e;
   }
 
