@@ -870,9 +870,9 @@ WorkPlan plan_work(const StageArgs<S> &a, int nsm, int *counter) {
   const int pl_p = wk.kz - a.kbeg, pl_i = a.kend - wk.kz;
   wk.nzc = pl_p > 0 ? (pl_p + 31) / 32 : 0;
   wk.chunk_p = wk.nzc ? (pl_p + wk.nzc - 1) / wk.nzc : 1;
-  // upper planes: about 24 items per SM, chunks of at least 24 planes
-  int nic = pl_i > 0 ? (24 * nsm * slots + tiles - 1) / tiles : 0;
-  if (pl_i > 0) nic = std::max(1, std::min(nic, pl_i / 24));
+  // upper planes: about 40 items per CTA slot, chunks of at least 16 planes
+  int nic = pl_i > 0 ? (40 * nsm * slots + tiles - 1) / tiles : 0;
+  if (pl_i > 0) nic = std::max(1, std::min(nic, pl_i / 16));
   wk.chunk_i = nic ? (pl_i + nic - 1) / nic : 1;
   wk.nic = nic ? (pl_i + wk.chunk_i - 1) / wk.chunk_i : 0;
   wk.nitems = 0;
