@@ -15,7 +15,8 @@
 //               halo of the one-sided stencils (x origin 16-byte aligned);
 //   C ring (2): the 9 metrics and (mu, lambda, buoyancy) of one output plane;
 //   M ring (2): the RK step state m and accumulator t of one output plane
-//               (stages that read them).
+//               (stages that read them);
+// (4/3/3 slots in the 16-bit PML variant, see Geo).
 // With 16-bit storage the interior variant converts each W plane to FP32 once
 // in shared memory (two plane buffers), so its stencils read FP32 like the
 // FP32 kernel instead of converting every tap.
