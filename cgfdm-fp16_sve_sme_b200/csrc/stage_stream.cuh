@@ -586,7 +586,11 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         constexpr int NE = 9 * BY * BX;
         static_assert(NE % 4 == 0, "conversion in groups of four");
         float *fd = (float *)(smem + G::OFF_F + (n & 1) * G::F_BYTES);
-        for (int e = 4 * tid; e < NE; e += 4 * NTHR) *(float4 *)(fd + e) = cvt4(tq + e);
+#pragma unroll
+        for (int g = 0; g < (NE + 4 * NTHR - 1) / (4 * NTHR); ++g) {
+          const int e = 4 * (tid + g * NTHR);
+          if (e < NE) *(float4 *)(fd + e) = cvt4(tq + e);
+        }
       }
 #pragma unroll
       for (int v = 0; v < 9; ++v) win[v][P0] = ldv(tq + (v * BY + ys) * BX + xs);
