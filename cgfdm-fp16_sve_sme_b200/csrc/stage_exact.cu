@@ -296,9 +296,11 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
 }  // namespace
 
 template <typename S> cudaError_t launch_stage_exact(const StageArgs<S> &a, cudaStream_t st) {
-  dim3 block(32, 4, 2);
+  // one plane per block: the three free-surface layers of the streaming path
+  // leave no thread idle, and a block's 8 rows share their y-neighbour rows
+  dim3 block(32, 8, 1);
   if (a.kend <= a.kbeg) return cudaSuccess;
-  dim3 grid((a.L.nx_ - 2 * HALO + 31) / 32, (a.L.ny_ - 2 * HALO + 3) / 4, (a.kend - a.kbeg + 1) / 2);
+  dim3 grid((a.L.nx_ - 2 * HALO + 31) / 32, (a.L.ny_ - 2 * HALO + 7) / 8, a.kend - a.kbeg);
   stage_exact_kernel<S><<<grid, block, 0, st>>>(a);
   return cudaGetLastError();
 }
