@@ -97,7 +97,9 @@ int cgfdm_create(const cgfdm_desc *desc, cgfdm_handle **out);
 int cgfdm_destroy(cgfdm_handle *h);
 
 /* Uploads the medium/metric coefficients and free-surface matrices in the
- * reference layout (the CJM and mat_rDZ arguments of propagate()). */
+ * reference layout (the CJM and mat_rDZ arguments of propagate()).  Waits for
+ * the handle's outstanding work first and returns once the upload is done;
+ * the RK accumulator is cleared (a stage 0 rewrites it before any read). */
 int cgfdm_set_model(cgfdm_handle *h, const float *cjm, const float *rdz);
 
 /* The smoothed explosive point source of singleSource.cpp:78-177 at padded
