@@ -5,8 +5,13 @@ over the whole grid of the workload.  Metric: grid-point updates per second
 per RK4 step (Gpt-updates/s).  Multi-GPU: independent replicas (the path is
 not sharded), weak scaling, max time over ranks.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3-1201]
                   [--precision fp32] [--impl ours|reference]
+
+The default workload is the 1201 x 1201 x 401 PerformanceTest shape in FP32
+with the scaled-FP16 form timed beside it; an accuracy block runs the
+Gaussian-hill configuration (401 x 401 x 201, 2000 steps) in FP64, FP32 and
+scaled FP16 and reports each one's relative L2 error against FP64.
 
 --impl reference times the reference's own scalar CPU build (oracle/_ref,
 compiled in place from the reference sources, run on all host cores as MPI
@@ -52,61 +57,12 @@ def log(*a):
 # --------------------------------------------------------------------------
 # workloads (synthetic inputs with the shapes of the benchmark configurations)
 # --------------------------------------------------------------------------
-C2_LAYERS = [(2.0, 2.6, 4.5, 2.3), (8.0, 3.35, 5.8, 2.6), (1000.0, 3.75, 6.5, 2.8)]
-
-
-def workload_c2(nsteps_total):
-    """401 x 401 x 201 Gaussian hill (1500 m at x = y = 20 km, 5 km width),
-    bottom at -20 km, three layers, 20-cell PML, explosive Ricker source
-    (f0 = 2 Hz) 3 km under the hill flank, 121 surface stations."""
-    NX, NY, NZ, DH = 401, 401, 201, 100.0
-    dt = 0.008
-    p = S.params(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=dt, TMAX=(nsteps_total + 0.5) * dt,
-                 **{"Depth(km)": 20.0}, centerX=0, centerY=0, nPML=20, useTerrain=1,
-                 useMedium=1, LayeredModel=1, rickerfc=2.0, IT_SKIP=10 ** 7, out="out")
-    terrain = S.gaussian_hill(p, amp=1500.0, x0=20000.0, y0=20000.0, width=5000.0)
-    # source at i=170, j=200, 3 km below the local surface
-    h = float(terrain[200 + 3, 170 + 3])
-    dz = (h + 20000.0) / (NZ - 1)
-    p.update(sourceX=170, sourceY=200, sourceZ=int(round(NZ - 1 - 3000.0 / dz)))
-    stations = {"S%03d" % (a * 11 + b): [50 + 30 * a, 50 + 30 * b, NZ - 1]
-                for a in range(11) for b in range(11)}
-    return {"name": "c2-gaussian-hill-401x401x201", "params": p, "stations": stations,
-            "terrain": terrain, "layers": S.layered_bytes(C2_LAYERS)}
-
-
-def workload_c3(n, nsteps_total):
-    """n x n x 401 PerformanceTest shape: seeded random terrain (500 m RMS,
-    10 km correlation), the C2 layers with a seeded +-5 % velocity
-    perturbation, an 80 x 40 point finite fault (40 x 20 km, strike 90,
-    dip 30, log-normal slip of mean 1.5 m, rupture at 0.8 Vs, Gaussian STF of
-    1 s)."""
-    NZ, DH, dt = 401, 100.0, 0.008
-    p = S.params(NX=n, NY=n, NZ=NZ, DH=DH, DT=dt, TMAX=(nsteps_total + 0.5) * dt,
-                 **{"Depth(km)": 40.0}, centerX=n // 2, centerY=n // 2, nPML=12,
-                 useTerrain=1, useMedium=1, LayeredModel=1, useMultiSource=1,
-                 **{"useSingleSource(ricker)": 0}, IT_SKIP=10 ** 7, out="out",
-                 mediumPerturbation=0.05, mediumSeed=3)
-    terrain = S.random_terrain(p, rms=500.0, corr=10000.0, seed=11)
-    fault_len = min(40000.0, (n - 40) * DH * 0.6)
-    fault_wid = fault_len / 2
-    nt_src = nsteps_total + 8
-    src = S.finite_fault(cx=0.0, cy=0.0, cz=-12000.0, length=fault_len, width=fault_wid,
-                         nl=80, nw=40, strike=90.0, dip=30.0, rake=90.0, mean_slip=1.5,
-                         vs_rupture=0.8 * 3350.0, stf_width=1.0, nt=nt_src, dt=dt, seed=5,
-                         surface_z=float(terrain.max()))
-    stations = {"S%03d" % (a * 11 + b): [n // 12 * (a + 1), n // 12 * (b + 1), NZ - 1]
-                for a in range(11) for b in range(11)}
-    return {"name": "c3-perftest-%dx%dx401" % (n, n), "params": p, "stations": stations,
-            "terrain": terrain, "layers": S.layered_bytes(C2_LAYERS), "source": src}
-
-
 def make_workload(name, nsteps_total):
     if name == "c2":
-        return workload_c2(nsteps_total)
+        return S.c2_workload(nsteps_total)
     m = re.fullmatch(r"c3-(\d+)", name)
     if m:
-        return workload_c3(int(m.group(1)), nsteps_total)
+        return S.c3_workload(int(m.group(1)), nsteps_total)
     raise SystemExit("unknown workload " + name)
 
 
@@ -172,9 +128,10 @@ class ClockSampler:
 # --------------------------------------------------------------------------
 def pick_decomposition(p, cores):
     """PX*PY*PZ <= cores with every rank at least max(nPML, 8) cells per axis
-    (init_grid.cpp:109-117), preferring the largest rank count."""
-    best = (1, 1, 1)
+    (init_grid.cpp:109-117): the largest rank count, and among those the
+    split with the fewest padded points (the least halo)."""
     lim = max(p["nPML"], 8)
+    best, best_key = (1, 1, 1), None
     for px in range(1, cores + 1):
         if p["NX"] // px < lim:
             break
@@ -184,29 +141,70 @@ def pick_decomposition(p, cores):
             for pz in range(1, cores // (px * py) + 1):
                 if p["NZ"] // pz < lim:
                     break
-                if px * py * pz > best[0] * best[1] * best[2]:
-                    best = (px, py, pz)
+                pad = (p["NX"] + 6 * px) * (p["NY"] + 6 * py) * (p["NZ"] + 6 * pz)
+                key = (px * py * pz, -pad)
+                if best_key is None or key > best_key:
+                    best, best_key = (px, py, pz), key
     return best
 
 
-def run_reference(w, nsteps, cores, timeout_s=900):
-    """Runs the reference on a copy of the workload for nsteps steps with
-    MPI ranks = cores; returns (seconds per step over the timed 10-step
-    blocks after the first, ranks used, steps timed)."""
+def reference_bytes(p, ranks):
+    """Host memory the reference holds during its time loop: 49 FLOAT fields
+    per padded point of every rank (13 CJM + 4 x 9 wavefield, run.cpp:63-96,
+    propagate.cpp:65-92) plus the PML auxiliaries (4 x 9 floats per slab
+    point), with each rank's halo counted."""
+    px, py, pz = ranks
+    padded = 0
+    for X in range(px):
+        nx = p["NX"] // px + (1 if X < p["NX"] % px else 0)
+        for Y in range(py):
+            ny = p["NY"] // py + (1 if Y < p["NY"] % py else 0)
+            for Z in range(pz):
+                nz = p["NZ"] // pz + (1 if Z < p["NZ"] % pz else 0)
+                padded += (nx + 6) * (ny + 6) * (nz + 6)
+    n = p["nPML"]
+    slab = 2 * n * p["NY"] * p["NZ"] + 2 * p["NX"] * n * p["NZ"] + p["NX"] * p["NY"] * n
+    return 4 * 49 * padded + 4 * 36 * slab
+
+
+def mem_available():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return None
+
+
+def run_reference(w, nsteps, cores, timeout_s=1500):
+    """Runs the reference on a copy of the workload with MPI ranks = cores
+    and returns (seconds per step, ranks used, steps timed).  The reference
+    prints a `Step time loss` line for step 0 and then one per 10 steps
+    (propagate.cpp:183-195); the per-step time is the mean of the 10-step
+    blocks after the first (nsteps >= 20), or of the one 10-step block after
+    step 0 (nsteps < 20, for grids whose steps take tens of seconds)."""
     if not os.path.exists(REF_EXE):
         raise RuntimeError("reference build missing at %s (make -C oracle ref)" % REF_EXE)
     p = dict(w["params"])
     dt = np.float32(p["DT"])
-    total = 10 * max(2, math.ceil(nsteps / 10)) + 1
+    nblocks = 1 if nsteps < 20 else max(2, math.ceil(nsteps / 10))
+    total = 10 * nblocks + 1
     p["TMAX"] = float((total + 0.5) * dt)
     px, py, pz = pick_decomposition(p, cores)
     p.update(PX=px, PY=py, PZ=pz)
+    need, avail = reference_bytes(p, (px, py, pz)), mem_available()
+    if avail is not None and need * 1.2 > avail:
+        raise RuntimeError("the reference needs about %.0f GB of host memory for %s on %d ranks, "
+                           "%.0f GB available" % (need / 1e9, w["name"], px * py * pz, avail / 1e9))
     d = tempfile.mkdtemp(prefix="cgfdm_ref_")
     try:
         ww = dict(w)
         ww["params"] = p
         write_workload(ww, d)
-        env = dict(os.environ, CGFDM_SHIM_NPROC=str(px * py * pz), CGFDM_SHIM_TIMEOUT="600")
+        env = dict(os.environ, CGFDM_SHIM_NPROC=str(px * py * pz),
+                   CGFDM_SHIM_TIMEOUT=str(timeout_s))
         r = subprocess.run([REF_EXE], cwd=d, env=env, capture_output=True, text=True,
                            timeout=timeout_s, start_new_session=True)
         if r.returncode != 0:
@@ -224,6 +222,17 @@ def run_reference(w, nsteps, cores, timeout_s=900):
         shutil.rmtree(d, ignore_errors=True)
 
 
+def cpu_sample_workload(name):
+    """The bounded CPU-baseline sample of a workload: the grid itself up to
+    401 x 401 x 401 points of columns, else the same generator at 401 x 401
+    columns (the reference's per-point cost does not depend on the grid
+    size; a 1201^2 step takes about half a minute on 16 cores)."""
+    m = re.fullmatch(r"c3-(\d+)", name)
+    if m and int(m.group(1)) > 401:
+        return "c3-401"
+    return name
+
+
 # --------------------------------------------------------------------------
 def _propagate(cgfdm, setup, prec, kern, device, nsteps):
     d0 = setup["desc"]
@@ -237,27 +246,38 @@ def _propagate(cgfdm, setup, prec, kern, device, nsteps):
         src_nt=setup["src_nt"], src_dt=setup["src_dt"], stations=setup["stations"])
 
 
-def measure_accuracy(cgfdm, w, prec, kern, device, nsteps, setup):
+def measure_accuracy(cgfdm, wname, nsteps, precisions, device):
     """Relative L2 error of the seismograms (Vx, Vy, Vz of every station over
-    all steps) and of the final free-surface velocity snapshot, against an
-    FP64 run of the same workload on the GPU."""
-    d = tempfile.mkdtemp(prefix="cgfdm_acc_")
-    try:
-        write_workload(w, d)
-        s64 = cgfdm.setup_from_directory(d, cgfdm.FP64)
-    finally:
-        shutil.rmtree(d, ignore_errors=True)
-    ref = _propagate(cgfdm, s64, cgfdm.FP64, cgfdm.KERNEL_AUTO, device, nsteps)
-    out = _propagate(cgfdm, setup, prec, kern, device, nsteps)
+    all steps) and of the final free-surface velocity snapshot of each
+    precision (the streaming kernels, KERNEL_AUTO) against an FP64 run of the
+    same workload on the GPU (the exact-order kernel templated on double),
+    all through propagate().  Returns {precision: {...}}."""
+    w = make_workload(wname, nsteps + 2)
     rel = lambda a, b: float(np.linalg.norm((a - b).ravel().astype(np.float64)) /
                              max(np.linalg.norm(b.ravel().astype(np.float64)), 1e-300))
-    nsta = ref[0].shape[0] if ref[0].ndim > 1 else len(setup["stations"])
-    sta_ref = ref[0].reshape(nsta, -1, 9)[:, :nsteps, :3]
-    sta_out = out[0].reshape(nsta, -1, 9)[:, :nsteps, :3]
-    return {"reference": "fp64 GPU run (same workload, same kernels templated on double)",
-            "steps": nsteps, "rel_l2_stations_v": rel(sta_out, sta_ref),
-            "rel_l2_free_surface_v": rel(out[2], ref[2]),
-            "max_abs_ref_v": float(np.abs(sta_ref).max())}
+
+    def run(prec):
+        d = tempfile.mkdtemp(prefix="cgfdm_acc_")
+        try:
+            write_workload(w, d)
+            st = cgfdm.setup_from_directory(d, prec)
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+        t0 = time.perf_counter()
+        sta, _, fs = _propagate(cgfdm, st, prec, cgfdm.KERNEL_AUTO, device, nsteps)
+        nsta = len(st["stations"])
+        return sta.reshape(nsta, -1, 9)[:, :nsteps, :3], fs, time.perf_counter() - t0
+
+    ref_sta, ref_fs, t64 = run(cgfdm.FP64)
+    out = {"workload": w["name"], "steps": nsteps,
+           "reference": "fp64 GPU run of the same workload (exact-order kernel on double)",
+           "fp64_seconds": t64, "max_abs_ref_v": float(np.abs(ref_sta).max())}
+    names = {cgfdm.FP32: "fp32", cgfdm.FP16: "fp16", cgfdm.BF16: "bf16"}
+    for prec in precisions:
+        sta, fs, _ = run(prec)
+        out[names[prec]] = {"rel_l2_stations_v": rel(sta, ref_sta),
+                            "rel_l2_free_surface_v": rel(fs, ref_fs)}
+    return out
 
 
 # --------------------------------------------------------------------------
@@ -445,7 +465,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--workload", default="c3-1201",
+                    help="c2, c3-N (N x N x 401), c4 (batched scenarios) or c5 (serving)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16", "bf16", "fp64"])
     ap.add_argument("--kernel", default="auto", choices=["auto", "exact", "stream"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -460,10 +481,13 @@ def main():
     ap.add_argument("--requests", type=int, default=32, help="requests of --workload c5")
     ap.add_argument("--step-scale", type=float, default=0.1,
                     help="--workload c5: request step counts are U[500, 3000] times this")
-    ap.add_argument("--accuracy-steps", type=int, default=0,
-                    help="also run this many steps in FP64 and in --precision through "
-                         "propagate() and report the relative L2 error of the station "
-                         "seismograms and the free-surface snapshot")
+    ap.add_argument("--accuracy-workload", default="c2",
+                    help="workload of the accuracy block (FP64 must fit one GPU)")
+    ap.add_argument("--accuracy-steps", type=int, default=2000,
+                    help="steps of the accuracy block: FP64, FP32 and scaled FP16 (and "
+                         "--precision) through propagate(), relative L2 of the station "
+                         "seismograms and the free-surface snapshot against FP64 "
+                         "(0: no accuracy block)"),
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -478,15 +502,20 @@ def main():
             return 0
         w = make_workload(args.workload, args.warmup + args.steps + 2)
         cores = os.cpu_count() or 1
+        npts_w = w["params"]["NX"] * w["params"]["NY"] * w["params"]["NZ"]
+        # grids whose reference steps take tens of seconds: step 0 and one
+        # timed 10-step block (a bounded sample of the run's steps)
+        ref_steps = args.warmup + args.steps if npts_w <= 1e8 else 10
         try:
-            sps, ranks, timed = run_reference(w, args.warmup + args.steps, cores)
+            sps, ranks, timed = run_reference(w, ref_steps, cores)
         except Exception as e:  # noqa: BLE001
             print(json.dumps({"impl": "reference", "unavailable": str(e)[:300]}))
             return 0
         npts = w["params"]["NX"] * w["params"]["NY"] * w["params"]["NZ"]
         v = npts / sps / 1e9
-        sample = "%s, %d timed steps (10-step blocks after a warm-up block), %d MPI ranks" % (
-            w["name"], timed, ranks)
+        sample = "%s (the whole grid), %d timed steps (%s), %d MPI ranks" % (
+            w["name"], timed, "10-step blocks after a warm-up block" if timed > 10 else
+            "one 10-step block after step 0", ranks)
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
             "steps": timed, "warmup": args.warmup, "ms_per_step": sps * 1e3,
@@ -524,7 +553,7 @@ def main():
             "stream": cgfdm.KERNEL_STREAM}[args.kernel]
 
     total_steps = args.warmup + args.steps
-    w = make_workload(args.workload, max(total_steps, args.e2e_steps, args.accuracy_steps) + 2)
+    w = make_workload(args.workload, max(total_steps, args.e2e_steps) + 2)
     d = tempfile.mkdtemp(prefix="cgfdm_bench_")
     write_workload(w, d)
     t0 = time.perf_counter()
@@ -608,8 +637,8 @@ def main():
     d2h = out_sta.nbytes + out_pgv.nbytes + out_fs.nbytes
 
     # the scaled-FP16 form on the same workload, timed the same way (the
-    # metric pairs it with FP32; its error against FP64 is the opt-in
-    # --accuracy-steps run)
+    # metric pairs it with FP32; its error against FP64 comes from the
+    # accuracy block below)
     fp16 = None
     if args.precision == "fp32" and not args.no_fp16:
         d16 = tempfile.mkdtemp(prefix="cgfdm_bench_")
@@ -644,13 +673,22 @@ def main():
         v16, ms16_max = replica_throughput(torch, dist, ms16 / 1e3, npts, args.steps, ws, "cuda")
         fp16 = {"value": v16, "unit": UNIT, "ms_per_step": ms16_max * 1e3 / args.steps,
                 "speedup_vs_fp32": v16 / value, "tile_rows": ks16["tile_rows"],
-                "bytes_per_point_step": BYTES_PER_POINT_STEP["fp16"],
-                "accuracy": "rel L2 vs the FP64 GPU run, C2 2000 steps: 4.7e-3 (seismograms); "
-                            "python bench.py --precision fp16 --accuracy-steps 2000"}
+                "bytes_per_point_step": BYTES_PER_POINT_STEP["fp16"]}
 
+    # error against FP64 of the precisions of this line, measured in this run
+    # on a workload whose FP64 form fits one GPU
     accuracy = None
-    if args.accuracy_steps > 0:
-        accuracy = measure_accuracy(cgfdm, w, prec, kern, local, args.accuracy_steps, setup)
+    if args.accuracy_steps > 0 and ws == 1:
+        precs = [prec] + ([cgfdm.FP16] if fp16 and prec != cgfdm.FP16 else [])
+        if prec == cgfdm.FP64:
+            precs = []
+        t0 = time.perf_counter()
+        accuracy = measure_accuracy(cgfdm, args.accuracy_workload, args.accuracy_steps, precs,
+                                    local)
+        accuracy["seconds"] = time.perf_counter() - t0
+        if fp16 and "fp16" in accuracy:
+            fp16["accuracy"] = dict(accuracy["fp16"], workload=accuracy["workload"],
+                                    steps=accuracy["steps"], against="fp64 GPU run")
 
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -692,11 +730,14 @@ def main():
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cw = make_workload(cpu_sample_workload(args.workload), 12)
         try:
-            sps, ranks, timed = run_reference(w, args.cpu_baseline_steps, os.cpu_count() or 1)
-            cpu = {"value": npts / sps / 1e9, "unit": UNIT, "cores": ranks, "kind": "reference",
-                   "sample": "%s, %d timed steps on %d MPI ranks (reference FP32 CPU build)" % (
-                       w["name"], timed, ranks)}
+            sps, ranks, timed = run_reference(cw, 10, os.cpu_count() or 1)
+            npc = cw["params"]["NX"] * cw["params"]["NY"] * cw["params"]["NZ"]
+            cpu = {"value": npc / sps / 1e9, "unit": UNIT, "cores": ranks, "kind": "reference",
+                   "sample": "%s, %d timed steps on %d MPI ranks (reference FP32 CPU build)%s" % (
+                       cw["name"], timed, ranks, "" if cw["name"] == w["name"] else
+                       "; a bounded sample of %s (same generator, fewer columns)" % w["name"])}
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                    "sample": "unavailable: %s" % str(e)[:200]}

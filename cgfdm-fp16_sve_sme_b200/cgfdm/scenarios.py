@@ -233,3 +233,61 @@ def sample_scenario(seed, nx_range=(121, 401), nz_range=(101, 201), points=None,
     return {"params": p, "terrain": terrain, "layers": layers, "source": src,
             "stations": stations}
 
+
+
+# --------------------------------------------------------------------------
+# the benchmark configurations
+# --------------------------------------------------------------------------
+C2_LAYERS = [(2.0, 2.6, 4.5, 2.3), (8.0, 3.35, 5.8, 2.6), (1000.0, 3.75, 6.5, 2.8)]
+
+
+def c2_workload(nsteps_total, it_skip=10 ** 7, slice_free_surf=0):
+    """401 x 401 x 201 Gaussian hill (1500 m at x = y = 20 km, 5 km width),
+    bottom at -20 km, three layers, 20-cell PML, explosive Ricker source
+    (f0 = 2 Hz, the single-source path) 3 km under the hill flank, 121
+    surface stations on an 11 x 11 lattice 3 km apart.  ``it_skip`` and
+    ``slice_free_surf`` ask for free-surface snapshots every it_skip steps."""
+    NX, NY, NZ, DH = 401, 401, 201, 100.0
+    dt = 0.008
+    p = params(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=dt, TMAX=(nsteps_total + 0.5) * dt,
+               **{"Depth(km)": 20.0}, centerX=0, centerY=0, nPML=20, useTerrain=1,
+               useMedium=1, LayeredModel=1, rickerfc=2.0, IT_SKIP=it_skip,
+               sliceFreeSurf=slice_free_surf, out="out")
+    terrain = gaussian_hill(p, amp=1500.0, x0=20000.0, y0=20000.0, width=5000.0)
+    # source at i=170, j=200, 3 km below the local surface
+    h = float(terrain[200 + HALO, 170 + HALO])
+    dz = (h + 20000.0) / (NZ - 1)
+    p.update(sourceX=170, sourceY=200, sourceZ=int(round(NZ - 1 - 3000.0 / dz)))
+    stations = {"S%03d" % (a * 11 + b): [50 + 30 * a, 50 + 30 * b, NZ - 1]
+                for a in range(11) for b in range(11)}
+    return {"name": "c2-gaussian-hill-401x401x201", "params": p, "stations": stations,
+            "terrain": terrain, "layers": layered_bytes(C2_LAYERS)}
+
+
+def c3_workload(n, nsteps_total, perturbation=0.05, it_skip=10 ** 7, slice_free_surf=0):
+    """n x n x 401 PerformanceTest shape (PerformanceTest/params.json_*):
+    seeded random terrain (500 m RMS, 10 km correlation), the C2 layers with
+    a seeded +-``perturbation`` velocity perturbation per cell (a host-setup
+    extension; the reference's own medium reader has none), a finite fault
+    of 80 x 40 points (40 x 20 km where the grid allows, strike 90, dip 30,
+    log-normal slip of mean 1.5 m, rupture at 0.8 Vs, Gaussian slip rate of
+    1 s), 121 surface stations."""
+    NZ, DH, dt = 401, 100.0, 0.008
+    extra = dict(mediumPerturbation=perturbation, mediumSeed=3) if perturbation else {}
+    p = params(NX=n, NY=n, NZ=NZ, DH=DH, DT=dt, TMAX=(nsteps_total + 0.5) * dt,
+               **{"Depth(km)": 40.0}, centerX=n // 2, centerY=n // 2, nPML=12,
+               useTerrain=1, useMedium=1, LayeredModel=1, useMultiSource=1,
+               **{"useSingleSource(ricker)": 0}, IT_SKIP=it_skip,
+               sliceFreeSurf=slice_free_surf, out="out", **extra)
+    terrain = random_terrain(p, rms=500.0, corr=10000.0, seed=11)
+    fault_len = min(40000.0, (n - 40) * DH * 0.6)
+    fault_wid = fault_len / 2
+    nt_src = nsteps_total + 8
+    src = finite_fault(cx=0.0, cy=0.0, cz=-12000.0, length=fault_len, width=fault_wid,
+                       nl=80, nw=40, strike=90.0, dip=30.0, rake=90.0, mean_slip=1.5,
+                       vs_rupture=0.8 * 3350.0, stf_width=1.0, nt=nt_src, dt=dt, seed=5,
+                       surface_z=float(terrain.max()))
+    stations = {"S%03d" % (a * 11 + b): [n // 12 * (a + 1), n // 12 * (b + 1), NZ - 1]
+                for a in range(11) for b in range(11)}
+    return {"name": "c3-perftest-%dx%dx401" % (n, n), "params": p, "stations": stations,
+            "terrain": terrain, "layers": layered_bytes(C2_LAYERS), "source": src}

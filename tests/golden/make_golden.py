@@ -1,8 +1,7 @@
 """Regenerates the golden fixtures in tests/golden/ from the reference itself.
 
-Test infrastructure.  Needs the reference sources (default /root/reference,
-override with CGFDM_REF_ROOT) and the in-place reference build made by
-``make -C oracle ref``.  It is never run by the tests; its outputs are
+Test infrastructure.  Needs the reference sources (their root is the first
+argument) and builds the reference in place with ``make -C oracle ref``.  It is never run by the tests; its outputs are
 committed so that the tests run without the reference.
 
 Fixtures
@@ -20,6 +19,16 @@ run_point_fp16.npz
     The point-source run through the reference's scalar FP16 build (outputs
     only; the inputs are those of run_point.npz).  The FP16 build overflows
     on the finite-fault run (non-finite seismograms), so it has no fixture.
+c2_hill.npz, c3_201.npz
+    The Gaussian-hill configuration (401 x 401 x 201, nPML 20, 121
+    stations, explosive source; 400 steps) and the 201 x 201 x 401
+    PerformanceTest shape (random terrain, layered medium, 80 x 40 finite
+    fault; 700 steps, without the per-cell medium perturbation, which the
+    reference's medium reader has no counterpart for) through the
+    reference's FP32 build on 8 MPI ranks (PZ = 1), the rank files merged:
+    the Vx/Vy/Vz seismograms of the stations, the PGV map and the last two
+    free-surface snapshots.  A multi-rank reference run equals the
+    single-rank one bit for bit (checked on run_fault.npz's inputs).
 run_point.npz, run_fault.npz
     Complete reference runs (main.cpp -> run.cpp -> propagate.cpp) of small
     configurations: a flat half-space with the smoothed explosive point
@@ -42,8 +51,7 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(REPO, "tests"))
 import scenarios  # noqa: E402
 
-REF_ROOT = os.environ.get("CGFDM_REF_ROOT", "/root/reference")
-REF_SRC = os.path.join(REF_ROOT, "src-new-FP32-SVE")
+REF_SRC = None  # set by main() from the reference root given on the command line
 REF_DIR = os.path.join(REPO, "oracle", "_ref")
 DFLAGS = ("-DXFAST -DFREE_SURFACE -DPML -DSOLVE_DISPLACEMENT -DTerrain_Smooth "
           "-DDealWithFirstLayer -DLayeredStructureTerrain -DStructureTerrain").split()
@@ -164,18 +172,114 @@ def c1_fixture():
         shutil.rmtree(work)
 
 
+def _split(n, parts, c):
+    """The reference's block decomposition (init_grid.cpp:30-73): the first
+    n % parts ranks get one cell more."""
+    b, r = divmod(n, parts)
+    return (c * (b + 1), b + 1) if c < r else (r * (b + 1) + (c - r) * b, b)
+
+
+def read_outputs_ranks(sc, outdir, px, py):
+    """The rank files of a PX x PY x 1 reference run merged into the
+    single-rank arrays of scenarios.read_outputs (station.cpp:382-405,
+    PGV.cpp:103-111, data_io.cpp:434-495)."""
+    p = sc["params"]
+    nt = scenarios.S.nt_of(p)
+    NX, NY = p["NX"], p["NY"]
+    rows = {}
+    for X in range(px):
+        for Y in range(py):
+            fn = os.path.join(outdir, "station_mpi_%d_%d_0.bin" % (X, Y))
+            if not os.path.exists(fn):
+                continue
+            raw = np.fromfile(fn, np.uint8)
+            n = raw.size // (12 + 36 * nt)
+            xyz = raw[:12 * n].view(np.int32).reshape(n, 3)
+            wave = raw[12 * n:].view(np.float32).reshape(n, nt, 9)
+            for q in range(n):
+                rows[tuple(int(v) for v in xyz[q])] = wave[q]
+    res = {"station_wave": np.stack([rows[tuple(v)] for v in sc["stations"].values()])}
+    pgv = np.zeros((NY, NX, 2), np.float32)
+    snaps = {}
+    for X in range(px):
+        x0, nx = _split(NX, px, X)
+        for Y in range(py):
+            y0, ny = _split(NY, py, Y)
+            tag = "%d_%d_0" % (X, Y)
+            pgv[y0:y0 + ny, x0:x0 + nx] = np.fromfile(
+                os.path.join(outdir, "PGV_Z_mpi_%s.bin" % tag), np.float32).reshape(ny, nx, 2)
+            for it in range(0, nt, p["IT_SKIP"]):
+                fz = os.path.join(outdir, "FreeSurfVz_%d_Z_mpi_%s.bin" % (it, tag))
+                if not os.path.exists(fz):
+                    continue
+                s = snaps.setdefault(it, np.zeros((3, NY, NX), np.float32))
+                for c, ch in enumerate("xyz"):
+                    s[c, y0:y0 + ny, x0:x0 + nx] = np.fromfile(os.path.join(
+                        outdir, "FreeSurfV%s_%d_Z_mpi_%s.bin" % (ch, it, tag)),
+                        np.float32).reshape(ny, nx)
+    res["pgv"] = pgv
+    its = sorted(snaps)
+    res["freesurf"] = np.stack([snaps[k] for k in its])
+    res["freesurf_its"] = np.array(its)
+    return res
+
+
+def bench_fixture(name, sc, px, py, keep_snaps=2):
+    """A benchmark-configuration run through the reference's FP32 build on
+    px * py MPI ranks (shared-memory shim); outputs merged across ranks."""
+    exe = os.path.join(REF_DIR, "cgfdm_ref_fp32")
+    work = tempfile.mkdtemp(prefix="cgfdm_golden_")
+    try:
+        p = dict(sc["params"], PX=px, PY=py, PZ=1)
+        scenarios.write_inputs(dict(sc, params=p), work)
+        env = dict(os.environ, CGFDM_SHIM_NPROC=str(px * py), CGFDM_SHIM_TIMEOUT="7200")
+        subprocess.check_call([exe], cwd=work, env=env, stdout=subprocess.DEVNULL)
+        res = read_outputs_ranks(sc, os.path.join(work, p["out"]), px, py)
+        out = {"params_json": np.array(json.dumps(sc["params"])),
+               "stations_json": np.array(json.dumps(sc["stations"])),
+               "out_station_v": res["station_wave"][:, :, :3].copy(),
+               "out_pgv": res["pgv"],
+               "out_freesurf": res["freesurf"][-keep_snaps:],
+               "out_freesurf_its": res["freesurf_its"][-keep_snaps:]}
+        np.savez_compressed(os.path.join(HERE, name), **out)
+    finally:
+        shutil.rmtree(work)
+
+
+FIXTURES = ["stage_small", "run_point", "run_fault", "c1_halfspace", "run_point_fp16",
+            "c2_hill", "c3_201"]
+
+
 def main():
+    """python make_golden.py REF_ROOT [fixture ...]: REF_ROOT is the
+    reference project's root (the directory holding src-new-FP32-SVE); with
+    no fixture names every fixture is regenerated."""
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py REF_ROOT [%s ...]" % " | ".join(FIXTURES))
+    ref_root = sys.argv[1]
+    global REF_SRC
+    REF_SRC = os.path.join(ref_root, "src-new-FP32-SVE")
     if not os.path.isdir(REF_SRC):
         sys.exit("reference sources not found at %s" % REF_SRC)
-    subprocess.check_call(["make", "-C", os.path.join(REPO, "oracle"), "ref", "-j8"],
-                          stdout=subprocess.DEVNULL)
+    want = sys.argv[2:] or FIXTURES
+    subprocess.check_call(["make", "-C", os.path.join(REPO, "oracle"), "ref", "-j8",
+                           "REF_ROOT=" + ref_root], stdout=subprocess.DEVNULL)
     exe = build_dumper()
-    stage_fixture(exe)
-    run_fixture("run_point.npz", scenarios.run_point(), exe)
-    run_fixture("run_fault.npz", scenarios.run_fault(), exe)
-    c1_fixture()
+    if "stage_small" in want:
+        stage_fixture(exe)
+    if "run_point" in want:
+        run_fixture("run_point.npz", scenarios.run_point(), exe)
+    if "run_fault" in want:
+        run_fixture("run_fault.npz", scenarios.run_fault(), exe)
+    if "c1_halfspace" in want:
+        c1_fixture()
     # (the FP16 build overflows on run_fault: its seismograms are not finite)
-    run_fixture_fp16("run_point_fp16.npz", scenarios.run_point())
+    if "run_point_fp16" in want:
+        run_fixture_fp16("run_point_fp16.npz", scenarios.run_point())
+    if "c2_hill" in want:
+        bench_fixture("c2_hill.npz", scenarios.c2_parity(), 4, 2)
+    if "c3_201" in want:
+        bench_fixture("c3_201.npz", scenarios.c3_201_parity(), 4, 2)
     print("golden fixtures written to", HERE)
 
 

@@ -108,6 +108,29 @@ def c1():
     return {"params": p, "stations": stations, "source": src}
 
 
+def c2_parity():
+    """The Gaussian-hill benchmark configuration (401 x 401 x 201, nPML 20,
+    121 stations, explosive source) for 400 steps (3.2 s: the wave is at
+    the surface and still in the domain), free-surface snapshots every 133
+    steps."""
+    w = S.c2_workload(400, it_skip=133, slice_free_surf=1)
+    w["params"]["TMAX"] = 400 * 0.008 + 0.0001
+    return {"params": w["params"], "stations": w["stations"], "terrain": w["terrain"],
+            "layers": as_u8(w["layers"])}
+
+
+def c3_201_parity():
+    """The 201 x 201 x 401 PerformanceTest shape (random terrain, layered
+    medium, 80 x 40 finite fault, nPML 12) for 700 steps (5.6 s: the
+    rupture's waves reach the surface), free-surface snapshots every 233
+    steps; without the per-cell medium perturbation, which the reference's
+    medium reader cannot express."""
+    w = S.c3_workload(201, 700, perturbation=0.0, it_skip=233, slice_free_surf=1)
+    w["params"]["TMAX"] = 700 * 0.008 + 0.0001
+    return {"params": w["params"], "stations": w["stations"], "terrain": w["terrain"],
+            "layers": as_u8(w["layers"]), "source": as_u8(w["source"])}
+
+
 def read_outputs(sc, outdir):
     """Reads the reference's single-rank outputs (station.cpp:382-405,
     PGV.cpp:103-111, data_io.cpp:323-495)."""

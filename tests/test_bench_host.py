@@ -39,3 +39,25 @@ def test_sampled_scenarios_follow_the_ranges():
     w = S.sample_scenario(1, points=2e6, nsteps=10)
     n = w["params"]["NX"] * w["params"]["NY"] * w["params"]["NZ"]
     assert 0.8e6 < n < 3e6
+
+
+def test_decomposition_prefers_the_least_halo():
+    # 16 ranks on the 1201 x 1201 x 401 grid: a 4 x 4 column split holds
+    # fewer padded points than z slabs
+    p = {"NX": 1201, "NY": 1201, "NZ": 401, "nPML": 12}
+    assert bench.pick_decomposition(p, 16) == (4, 4, 1)
+
+
+def test_reference_memory_estimate_counts_every_rank_halo():
+    p = {"NX": 100, "NY": 60, "NZ": 40, "nPML": 10}
+    one = bench.reference_bytes(p, (1, 1, 1))
+    assert one == 4 * 49 * 106 * 66 * 46 + 4 * 36 * (2 * 10 * 60 * 40 + 2 * 100 * 10 * 40 +
+                                                      100 * 60 * 10)
+    # splitting x in two adds one 6-cell halo
+    assert bench.reference_bytes(p, (2, 1, 1)) - one == 4 * 49 * 6 * 66 * 46
+
+
+def test_cpu_baseline_sample_of_large_grids():
+    assert bench.cpu_sample_workload("c3-1201") == "c3-401"
+    assert bench.cpu_sample_workload("c3-401") == "c3-401"
+    assert bench.cpu_sample_workload("c2") == "c2"
