@@ -20,17 +20,22 @@
 //              when the kernel starts; every call zeroes it (cudaMemsetAsync on
 //              the caller's stream) before every launch.
 //   [256, ...) PML profiles alpha, beta, d for x, y, z (3 x (_nx_+_ny_+_nz_)
-//              floats), rewritten by every call before its launches.
+//              floats), rewritten by every call before its launches.  The
+//              values travel in the parameters of small fill kernels on the
+//              caller's stream (no host-to-device copy from pageable memory,
+//              which could block the host), so a call only enqueues work.
 // A grid whose profile table does not fit (nx + ny + nz + 18 > 5440) is
 // rejected with CGFDM_ERR_ARG.  Because all calls on a device share the
 // scratch, calls whose work overlaps on the GPU (different streams or host
 // threads) race.  The first call on a device resolves the scratch address
 // with cudaGetSymbolAddress (the array's name in host code is only a host
-// stand-in, never a device address) and sets kernel attributes; make that
-// first call before any stream capture.
+// stand-in, never a device address); make that first call before any stream
+// capture.  Each streaming-kernel variant has its shared-memory attribute set
+// on its first launch in the process.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -63,6 +68,30 @@ cudaError_t scratch_of(int dev, unsigned char **out) {
     g_addr[dev] = p;
   }
   *out = g_addr[dev];
+  return cudaSuccess;
+}
+
+// Fill kernel for the profile table: its values arrive in the kernel's
+// parameter space (at most 32 KB), copied by the launch itself.
+constexpr int kFillChunk = 7936;
+struct FillChunk {
+  int n;
+  float v[kFillChunk];
+};
+__global__ void fill_profile_kernel(float *dst, const __grid_constant__ FillChunk c) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < c.n; q += gridDim.x * blockDim.x)
+    dst[q] = c.v[q];
+}
+
+cudaError_t upload_profiles(float *dst, const std::vector<float> &prof, cudaStream_t st) {
+  static thread_local FillChunk c;
+  for (size_t q0 = 0; q0 < prof.size(); q0 += kFillChunk) {
+    c.n = (int)std::min<size_t>(kFillChunk, prof.size() - q0);
+    std::memcpy(c.v, prof.data() + q0, sizeof(float) * c.n);
+    fill_profile_kernel<<<(c.n + 255) / 256, 256, 0, st>>>(dst + q0, c);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   return cudaSuccess;
 }
 
@@ -116,24 +145,24 @@ int stage_noalloc(const cgfdm_stage_buffers &b, cudaStream_t st, unsigned char *
     off += 9LL * n[0] * n[1] * n[2];
     big = std::max(big, 9LL * n[0] * n[1] * n[2]);
   }
-  // the profile table is rewritten by every call (host copy is staged by the
-  // runtime before cudaMemcpyAsync returns, so the vector may go out of scope)
-  const std::vector<float> prof = pml_profiles(b.nx, b.ny, b.nz, b.npml, b.dh);
-  NA_TRY(cudaMemcpyAsync(scratch + kProfileOffset, prof.data(), sizeof(float) * prof.size(),
-                         cudaMemcpyHostToDevice, st));
-  alignas(64) unsigned char maps[kStreamMapsBytes];
-  int rc = encode_stream_maps<S>(a.win, a.cjm, a.wm, a.t, L, maps);
-  if (rc) return rc;
+  // the profile table is rewritten by every call, through kernel parameters
+  NA_TRY(upload_profiles((float *)(scratch + kProfileOffset),
+                         pml_profiles(b.nx, b.ny, b.nz, b.npml, b.dh), st));
   int *err = (int *)scratch, *counter = (int *)(scratch + 4);
   // as a handle does: the exact-order kernel alone when opposite PML slabs
   // overlap (nPML above half the grid) or a slab is too large for the
   // streaming kernel's 32-bit auxiliary offsets
   const bool overlap = b.npml > 0 && (2 * b.npml > b.nx || 2 * b.npml > b.ny || big >= (1LL << 32));
   const int ksurf = overlap ? HALO : L.nz_ - HALO - 3;
-  StageArgs<S> lower = a;
-  lower.kbeg = HALO;
-  lower.kend = ksurf;
-  NA_TRY(launch_stage_stream<S>(lower, maps, err, counter, st));
+  if (ksurf > HALO) {  // the streaming launch has planes: it needs the tensor maps
+    alignas(64) unsigned char maps[kStreamMapsBytes];
+    int rc = encode_stream_maps<S>(a.win, a.cjm, a.wm, a.t, L, maps);
+    if (rc) return rc;
+    StageArgs<S> lower = a;
+    lower.kbeg = HALO;
+    lower.kend = ksurf;
+    NA_TRY(launch_stage_stream<S>(lower, maps, err, counter, st));
+  }
   a.kbeg = ksurf;
   a.kend = L.nz_ - HALO;
   NA_TRY(launch_stage_exact<S>(a, st));
@@ -159,6 +188,17 @@ extern "C" int cgfdm_stage_noalloc(const cgfdm_stage_buffers *b, void *stream, i
     return fail(CGFDM_ERR_ARG, "a wavefield, coefficient or rDZ pointer is null");
   if (b->npml > 0 && (!b->aux_in || !b->aux_out || !b->aux_m || !b->aux_t))
     return fail(CGFDM_ERR_ARG, "nPML > 0 needs the four auxiliary buffers");
+  {
+    const void *ptrs[] = {b->w_in, b->w_out, b->w_m, b->t, b->cjm, b->rdz,
+                          b->aux_in, b->aux_out, b->aux_m, b->aux_t};
+    const char *names[] = {"w_in", "w_out", "w_m", "t", "cjm", "rdz",
+                           "aux_in", "aux_out", "aux_m", "aux_t"};
+    for (int q = 0; q < 10; ++q)
+      if (ptrs[q] && ((uintptr_t)ptrs[q] & 255u))
+        return fail(CGFDM_ERR_ARG, std::string(names[q]) +
+                                       " is not 256-byte aligned (the streaming kernel's tensor "
+                                       "maps and aligned rows need cudaMalloc alignment)");
+  }
   const long long need =
       kProfileOffset + 3LL * sizeof(float) * ((b->nx + 6LL) + (b->ny + 6LL) + (b->nz + 6LL));
   if (need > kScratchBytes)

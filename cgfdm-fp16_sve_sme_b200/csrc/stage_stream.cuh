@@ -42,6 +42,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -811,34 +812,48 @@ __global__ void __launch_bounds__(TX * 16, 1)
   stream_body<S, 16, FB1, FB2, FB3, PMLK, RK>(BatchSrc<S>{p}, err);
 }
 
+// Sets a kernel's dynamic shared-memory limit once per device.  `done` is
+// the kernel variant's own bit set of devices that have it; the attribute
+// call is idempotent, so two host threads that race here both make it and
+// both set the bit.
+template <typename K>
+cudaError_t ensure_smem_attr(K kern, int smem, std::atomic<unsigned long long> &done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+  return e;
+}
+
 template <typename S, int TYv, int FB1, int FB2, int FB3, bool PMLK, int RK>
 cudaError_t launch_variant(const StageArgs<S> &a, const Maps &maps, const Work &wk, int *err,
                            int nsm, cudaStream_t st) {
   using G = Geo<S, TYv, PMLK>;
-  static int attr_dev = -1;
+  static std::atomic<unsigned long long> attr_done{0};
   auto kern = stage_stream_kernel<S, TYv, FB1, FB2, FB3, PMLK, RK>;
   const int smem = G::SMEM;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (attr_dev != dev) {
-    cudaError_t e =
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    attr_dev = dev;
-  }
-  cudaError_t e = cudaMemsetAsync(wk.counter, 0, sizeof(int), st);
+  cudaError_t e = ensure_smem_attr(kern, smem, attr_done);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(wk.counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   kern<<<std::min(wk.nitems, nsm * G::MINB), G::NTHR, smem, st>>>(maps, a, wk, err);
   return cudaGetLastError();
 }
 
+// SM count of the current device, cached per device (atomics: handles may be
+// driven from several host threads).
 int sm_count() {
-  static int nsm = 0;
-  if (!nsm) {
-    int dev = 0;
-    cudaGetDevice(&dev);
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int nsm = dev >= 0 && dev < 64 ? cache[dev].load(std::memory_order_relaxed) : 0;
+  if (nsm <= 0) {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (nsm <= 0) nsm = 148;
+    if (dev >= 0 && dev < 64) cache[dev].store(nsm, std::memory_order_relaxed);
   }
   return nsm;
 }
@@ -914,18 +929,12 @@ cudaError_t launch_batch_variant(const BatchParams<S> &p, int items, int *err, i
                                  cudaStream_t st) {
   using G = Geo<S, 16, PMLK>;
   static_assert(sizeof(BatchParams<S>) <= 32000, "kernel parameter space");
-  static int attr_dev = -1;
+  static std::atomic<unsigned long long> attr_done{0};
   auto kern = stage_stream_batch_kernel<S, FB1, FB2, FB3, PMLK, RK>;
   const int smem = G::SMEM;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (attr_dev != dev) {
-    cudaError_t e =
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    attr_dev = dev;
-  }
-  cudaError_t e = cudaMemsetAsync(p.counter, 0, sizeof(int), st);
+  cudaError_t e = ensure_smem_attr(kern, smem, attr_done);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(p.counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   kern<<<std::min(items, nsm), G::NTHR, smem, st>>>(p, err);
   return cudaGetLastError();
@@ -977,15 +986,16 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
+  // resolved once (a function-local static is initialised thread-safely)
+  static const EncodeTiledFn fn = []() -> EncodeTiledFn {
     void *p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
             cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = (EncodeTiledFn)p;
-  }
+      return (EncodeTiledFn)p;
+    return nullptr;
+  }();
   return fn;
 }
 template <typename S> CUtensorMapDataType dtype_of();

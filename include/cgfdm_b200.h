@@ -124,7 +124,9 @@ int cgfdm_set_stations(cgfdm_handle *h, const int32_t *xyz, int32_t nsta);
 int cgfdm_run(cgfdm_handle *h, int32_t nsteps, void *stream);
 
 /* One RK stage irk (0..3) with MacCormack signs fb1..fb3 and no source,
- * station or PGV work: the unit of the stage-level parity tests. */
+ * station or PGV work: the unit of the stage-level parity tests.  Stages 1-3
+ * read the RK accumulator that stage 0 (or cgfdm_set_state) left; a
+ * cgfdm_set_model call in between clears it (see cgfdm_set_state). */
 int cgfdm_stage(cgfdm_handle *h, int32_t irk, int32_t fb1, int32_t fb2, int32_t fb3,
                 void *stream);
 
@@ -146,7 +148,10 @@ int cgfdm_get_free_surface(cgfdm_handle *h, float *v3);
  * and (for irk 1..3) the step-start state m, each 9 x num; PML auxiliaries as
  * 5 slabs (x1 y1 z1 x2 y2) x {Aux, t, m}, each [npos][9]
  * (pml_deriv.cpp:12-32).  get_state returns the last stage's output W, t and
- * m (m is the stage input for irk 0, as the reference's m_W copy). */
+ * m (m is the stage input for irk 0, as the reference's m_W copy).
+ * Ordering: cgfdm_set_model stages its upload through the RK accumulator and
+ * clears it afterwards, so call it before cgfdm_set_state -- a t set for a
+ * stage irk > 0 and followed by cgfdm_set_model is lost. */
 int cgfdm_set_state(cgfdm_handle *h, int32_t irk, const float *W, const float *t,
                     const float *m, const float *aux);
 int cgfdm_get_state(cgfdm_handle *h, float *W, float *t, float *m, float *aux);
@@ -316,8 +321,12 @@ int cgfdm_server_destroy(cgfdm_server *s);
  * expired bounded wait, and is read and cleared only when `wait` is
  * non-zero: then the call synchronizes `stream` and returns CGFDM_ERR_TIMEOUT
  * if it was set.  With wait = 0 the call only enqueues work on `stream`
- * (current device).  The first call on a device resolves the scratch address
- * and kernel attributes; make it before any stream capture.
+ * (current device): the profile table reaches the scratch through the
+ * parameters of small fill kernels, not through a host-to-device copy.  The
+ * first call on a device resolves the scratch address; make it before any
+ * stream capture.  Each streaming-kernel variant has its shared-memory
+ * attribute set on its first launch in the process.  A pointer that is not
+ * 256-byte aligned is rejected with CGFDM_ERR_ARG.
  */
 typedef struct {
   int32_t nx, ny, nz, npml;
