@@ -471,8 +471,10 @@ def main():
     ap.add_argument("--kernel", default="auto", choices=["auto", "exact", "stream"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=100)
-    ap.add_argument("--tile-rows", type=int, default=0, choices=[0, 8, 16],
-                    help="streaming-kernel tile height (0: the library's autotuner)")
+    ap.add_argument("--tile-rows", type=int, default=0, choices=[0, 8, 16, 64],
+                    help="streaming-kernel tile form: 16 or 8 (32-column tiles of that height), "
+                         "64 (paired-point 64 x 8 tiles, FP16 / BF16), 0: the library's "
+                         "autotuner")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp16", action="store_true",
                     help="skip the scaled-FP16 companion measurement of an FP32 run")

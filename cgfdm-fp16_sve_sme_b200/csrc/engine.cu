@@ -634,8 +634,9 @@ template <typename S> class EngineT : public Engine {
   int set_timing(bool on) override { timing_ = on; return CGFDM_OK; }
 
   int set_tile_rows(int rows) override {
-    if (rows != 0 && rows != 8 && rows != 16) {
-      set_error("tile rows must be 0 (autotune), 8 or 16");
+    if (rows != 0 && rows != 8 && rows != 16 && !(rows == kTilePair && sizeof(S) == 2)) {
+      set_error("tile form must be 0 (autotune), 8 or 16 (32-column tiles of that height), or "
+                "64 (paired-point 64 x 8 tiles, FP16 / BF16 storage only)");
       return CGFDM_ERR_ARG;
     }
     tile_rows_ = rows;
@@ -753,7 +754,8 @@ template <typename S> class EngineT : public Engine {
     return a;
   }
 
-  // Picks the streaming kernel's tile height for this grid and precision:
+  // Picks the streaming kernel's tile form for this grid and precision (32 x
+  // 16, 32 x 8, and for 16-bit storage the paired-point 64 x 8 form):
   // times stage 0 at the current step boundary with each candidate (stage 0
   // reads only the step state and writes buffers the next stage 0 rewrites)
   // and keeps the fastest; results are cached per (precision, grid).
@@ -777,7 +779,9 @@ template <typename S> class EngineT : public Engine {
     int best = 16;
     float best_ms = 1e30f;
     cudaError_t err = cudaSuccess;
-    for (int rows : {16, 8}) {
+    std::vector<int> forms = {16, 8};
+    if (sizeof(S) == 2) forms.push_back(kTilePair);
+    for (int rows : forms) {
       err = launch_stage_stream<S>(b, tmap_[0], err_flag_, err_flag_ + 1, st, nullptr, nullptr,
                                    rows);
       if (err == cudaSuccess) err = cudaEventRecord(e0, st);

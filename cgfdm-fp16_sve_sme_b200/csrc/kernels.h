@@ -22,11 +22,16 @@ template <typename S> cudaError_t launch_stage_exact(const StageArgs<S> &a, cuda
 // TMA-staged z-streaming fused stage over kbeg <= k < kend, which must lie
 // below the three free-surface layers.  `maps` holds the tensor maps of the
 // stage input wavefield and of the coefficients (encode_stream_maps).
-constexpr int kStreamMapsBytes = 1280;
+constexpr int kStreamMapsBytes = 2048;
+// Tile form code of the paired-point kernel (16-bit storage): 64 x 8 tiles,
+// two x-adjacent points per thread.
+constexpr int kTilePair = 64;
 // `after_main` (optional) is recorded right after the streaming kernel,
 // before the exact-order kernel; `nlaunch` (optional) is increased by the
-// number of kernels launched; `tile_rows` (16 or 8) selects the tile height
-// (32 x 16 tiles, one CTA per SM; or 32 x 8, two CTAs per SM).
+// number of kernels launched; `tile_rows` selects the tile form: 16 (32 x 16
+// tiles, one CTA per SM), 8 (32 x 8, two CTAs per SM) or kTilePair (16-bit
+// storage: the paired-point kernel on 64 x 8 interior tiles, the 32 x 8 PML
+// variant elsewhere).
 template <typename S>
 cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps, int *err_flag,
                                 int *work_counter, cudaStream_t st,

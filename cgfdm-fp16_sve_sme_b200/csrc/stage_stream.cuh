@@ -313,6 +313,7 @@ struct Maps {
 };
 struct MapSet {
   Maps ty16, ty8;  // the same buffers, boxes for tile heights 16 and 8
+  Maps pair;       // 16-bit storage: 64 x 8 tiles of the paired-point kernel
 };
 
 // Work items of one launch.  The z range [kbeg, kend) is cut at kz, the top
@@ -812,6 +813,318 @@ __global__ void __launch_bounds__(TX * 16, 1)
   stream_body<S, 16, FB1, FB2, FB3, PMLK, RK>(BatchSrc<S>{p}, err);
 }
 
+// ---------------------------------------------------------------------------
+// 16-bit storage, interior items: the paired-point kernel.
+//
+// A 64 x 8 column tile per item and 256 threads, each owning two x-adjacent
+// points (columns i and i + 1, i - HALO even), so that every shared-memory
+// read, conversion and global store of the tile moves one 32-bit pair of
+// 16-bit values and the arithmetic of the two points is one packed FP32x2
+// instruction.  Per point and stage this issues about half the instructions
+// of the one-point 16-bit kernel, whose interior launches are bound by
+// instruction issue rather than by HBM.  The per-point arithmetic (operands,
+// operation order, rounding) is that of the one-point kernel's interior
+// variant, so both give the same bits.  Rings: W 4 slots (9 fields x 12 rows
+// x 80 columns: the tile, a 16-byte aligned 8-column halo on each side and
+// the y halo), coefficients 3 slots, m / t 3 slots; one CTA per SM.
+template <typename S> struct PairGeo {
+  static constexpr int TY = 8, TXP = 64, NTHR = 256, PLANE = TY * TXP;
+  static constexpr int BY = TY + 4, BX = 8 + TXP + 8;
+  static constexpr int W_BYTES = ((9 * BY * BX * 2) + 127) / 128 * 128;
+  static constexpr int C_BYTES = 12 * PLANE * 2;
+  static constexpr int M_BYTES = 18 * PLANE * 2;
+  static constexpr int NW = 4, NC = 3, NM = 3;
+  static constexpr int OFF_C = NW * W_BYTES;
+  static constexpr int OFF_M = OFF_C + NC * C_BYTES;
+  static constexpr int OFF_BAR = OFF_M + NM * M_BYTES;
+  static constexpr int SMEM = OFF_BAR + 8 * (NW + NC + NM) + 128;
+  static_assert(sizeof(S) == 2, "the paired-point kernel is for 16-bit storage");
+  static_assert(SMEM <= 232448, "shared memory budget");
+};
+
+// Two adjacent 16-bit values (4-byte aligned) as a float2, and back.
+__device__ __forceinline__ float2 ld2(const __half *p) { return __half22float2(*(const __half2 *)p); }
+__device__ __forceinline__ float2 ld2(const __nv_bfloat16 *p) {
+  return __bfloat1622float2(*(const __nv_bfloat162 *)p);
+}
+__device__ __forceinline__ void st2(__half *p, float2 v) { *(__half2 *)p = __float22half2_rn(v); }
+__device__ __forceinline__ void st2(__nv_bfloat16 *p, float2 v) {
+  *(__nv_bfloat162 *)p = __float22bfloat162_rn(v);
+}
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
+// ElasticSum for two points at once (lane x: point i, lane y: point i + 1),
+// the same operations in the same order.
+struct ElasticSum2 {
+  float2 v0, v1, v2, nx, ny, nz, s6, s7, s8;
+  template <bool FIRST>
+  __device__ __forceinline__ void add(const float2 m[3], float2 g, const float2 L[9]) {
+    const float2 a0 = f2mul(g, m[0]), a1 = f2mul(g, m[1]), a2 = f2mul(g, m[2]);
+    v0 = f2fma(a2, L[7], f2fma(a1, L[6], FIRST ? f2mul(a0, L[3]) : f2fma(a0, L[3], v0)));
+    v1 = f2fma(a2, L[8], f2fma(a1, L[4], FIRST ? f2mul(a0, L[6]) : f2fma(a0, L[6], v1)));
+    v2 = f2fma(a2, L[5], f2fma(a1, L[8], FIRST ? f2mul(a0, L[7]) : f2fma(a0, L[7], v2)));
+    nx = FIRST ? f2mul(a0, L[0]) : f2fma(a0, L[0], nx);
+    ny = FIRST ? f2mul(a1, L[1]) : f2fma(a1, L[1], ny);
+    nz = FIRST ? f2mul(a2, L[2]) : f2fma(a2, L[2], nz);
+    s6 = f2fma(a0, L[1], FIRST ? f2mul(a1, L[0]) : f2fma(a1, L[0], s6));
+    s7 = f2fma(a0, L[2], FIRST ? f2mul(a2, L[0]) : f2fma(a2, L[0], s7));
+    s8 = f2fma(a1, L[2], FIRST ? f2mul(a2, L[1]) : f2fma(a2, L[1], s8));
+  }
+  __device__ __forceinline__ void finish(float2 mu, float2 lam, float2 b, float2 h[9]) const {
+    h[0] = f2mul(v0, b);
+    h[1] = f2mul(v1, b);
+    h[2] = f2mul(v2, b);
+    const float2 div = f2mul(f2add(f2add(nx, ny), nz), lam), tmu = f2mul(pk(2.0f), mu);
+    h[3] = f2fma(tmu, nx, div);
+    h[4] = f2fma(tmu, ny, div);
+    h[5] = f2fma(tmu, nz, div);
+    h[6] = f2mul(s6, mu);
+    h[7] = f2mul(s7, mu);
+    h[8] = f2mul(s8, mu);
+  }
+};
+
+// Interior items of a paired launch: 64 x 8 tiles (two 32-column tiles of
+// the Work grid, starting at bx_lo; bx_hi - bx_lo is even) x the upper z
+// chunks, tiles fastest.
+__device__ __forceinline__ void item_of_pair(const Work &w, int item, int &pxi, int &byi, int &kb,
+                                             int &ke, int kend) {
+  const int npx = (w.bx_hi - w.bx_lo) / 2, ti = npx * (w.by_hi - w.by_lo);
+  const int t = item % ti, chk = item / ti;
+  pxi = t % npx;
+  byi = w.by_lo + t / npx;
+  kb = w.kz + chk * w.chunk_i;
+  ke = min(kb + w.chunk_i, kend);
+}
+
+template <typename S, int FB1, int FB2, int FB3, int RK>
+__global__ void __launch_bounds__(256, 1)
+    stage_pair_kernel(const __grid_constant__ Maps maps, const __grid_constant__ StageArgs<S> a,
+                      const __grid_constant__ Work wk, int *err) {
+  using G = PairGeo<S>;
+  constexpr int TY = G::TY, PLANE = G::PLANE, BY = G::BY, BX = G::BX;
+  constexpr int NW = G::NW, NC = G::NC, NM = G::NM;
+  constexpr int DIR = -FB3;  // sweep direction in z
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  uint64_t *bw = (uint64_t *)(smem + G::OFF_BAR);
+  uint64_t *bc = bw + NW;
+  uint64_t *bm = bc + NC;
+  __shared__ int s_item, s_bad;
+
+  const int tid = threadIdx.x;
+  const int c = tid % 32, r = tid / 32;
+  const int cidx = r * G::TXP + 2 * c;  // the pair's first element in a C / M plane
+
+  if (tid == 0) {
+    s_bad = 0;
+    for (int q = 0; q < NW + NC + NM; ++q) mbar_init(smem_u32(&bw[q]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  unsigned fw0 = 0, fc0 = 0, fm0 = 0;  // ring fill counters, continued across items
+  const Layout L = a.L;
+  constexpr bool need_m = RK == 1, need_t = RK >= 1;
+  const float cB = a.irk == 2 ? kB3 : kB2, cA = a.irk == 2 ? 1.0f : kA3rk;
+  const uint32_t m_bytes = ((need_m ? 9 : 0) + (need_t ? 9 : 0)) * PLANE * 2;
+  const float rDH = a.rDH, DT = a.DT;
+  const float gx = FB1 * rDH, gy = FB2 * rDH, gz = FB3 * rDH;
+  const float *px = a.pml, *py = a.pml + 3 * L.nx_, *pz = a.pml + 3 * L.nx_ + 3 * L.ny_;
+  const long long fs = L.fs;
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(wk.counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= wk.nitems || s_bad) break;
+    int pxi, byi, kb, ke;
+    item_of_pair(wk, item, pxi, byi, kb, ke, a.kend);
+    const int nout = ke - kb, nplanes = nout + 4;
+    const int q0 = DIR > 0 ? kb - 3 : ke + 2;  // input planes q_n = q0 + n*DIR
+    const int x0 = HALO + 32 * (wk.bx_lo + 2 * pxi);  // padded index of the tile's column 0
+    const int i = x0 + 2 * c, j = HALO + byi * TY + r;
+    const int tx0 = L.xoff + x0;  // HBM x of the tile's first column
+    const int wx0 = tx0 - 8;
+    const int wy0 = HALO + byi * TY - (FB2 > 0 ? 1 : 3);
+    const int ty0 = HALO + byi * TY;
+    const int xs = 2 * c + 8, ys = r + (FB2 > 0 ? 1 : 3);
+
+    auto issue_w = [&](int n) {
+      if (a.drop_one_load && item == 0 && n == NW - 1) return;  // test hook, see StageArgs
+      const unsigned f = fw0 + n, q = f % NW;
+      const uint32_t bar = smem_u32(&bw[q]);
+      mbar_expect_tx(bar, 9 * BY * BX * 2);
+      tma_load_4d(smem_u32(smem + q * G::W_BYTES), &maps.w, wx0, wy0, q0 + n * DIR, 0, bar);
+    };
+    auto issue_c = [&](int o) {  // output o is plane kb + o (DIR > 0) or ke-1-o
+      const unsigned f = fc0 + o, q = f % NC;
+      const int k = DIR > 0 ? kb + o : ke - 1 - o;
+      const uint32_t bar = smem_u32(&bc[q]);
+      unsigned char *dst = smem + G::OFF_C + q * G::C_BYTES;
+      mbar_expect_tx(bar, G::C_BYTES);
+      tma_load_4d(smem_u32(dst), &maps.c9, tx0, ty0, k, 0, bar);
+      tma_load_4d(smem_u32(dst + 9 * PLANE * 2), &maps.c3, tx0, ty0, k, 10, bar);
+    };
+    auto issue_m = [&](int o) {
+      const unsigned f = fm0 + o, q = f % NM;
+      const int k = DIR > 0 ? kb + o : ke - 1 - o;
+      const uint32_t bar = smem_u32(&bm[q]);
+      unsigned char *dst = smem + G::OFF_M + q * G::M_BYTES;
+      mbar_expect_tx(bar, m_bytes);
+      if (need_m) tma_load_4d(smem_u32(dst), &maps.m, tx0, ty0, k, 0, bar);
+      if (need_t) tma_load_4d(smem_u32(dst + 9 * PLANE * 2), &maps.t, tx0, ty0, k, 0, bar);
+    };
+    if (tid == 0) {
+      for (int n = 0; n < NW - 1 && n < nplanes; ++n) issue_w(n);
+      for (int o = 0; o < NC && o < nout; ++o) issue_c(o);
+      if (need_t)
+        for (int o = 0; o < NM && o < nout; ++o) issue_m(o);
+    }
+
+    // per-column PML beta times DT, with the direction's sign and 1/DH
+    const float2 bxd = make_float2(px[L.nx_ + i] * DT * gx, px[L.nx_ + i + 1] * DT * gx);
+    const float2 byd = pk(py[L.ny_ + j] * DT * gy);
+
+    float2 win[9][5];
+#pragma unroll
+    for (int v = 0; v < 9; ++v)
+#pragma unroll
+      for (int m = 0; m < 5; ++m) win[v][m] = pk(0.0f);
+
+    auto iter = [&](auto Rc, const int n) -> bool {
+      constexpr int R = decltype(Rc)::value;
+      constexpr int P0 = R, P1 = (R + 4) % 5, P2 = (R + 3) % 5, P3 = (R + 2) % 5, P4 = (R + 1) % 5;
+      const int o = n - 4;
+      bool ok = mbar_wait_bounded(smem_u32(&bw[(fw0 + n) % NW]), ((fw0 + n) / NW) & 1);
+      if (o >= 0) {
+        ok = ok && mbar_wait_bounded(smem_u32(&bc[(fc0 + o) % NC]), ((fc0 + o) / NC) & 1);
+        if (need_t) ok = ok && mbar_wait_bounded(smem_u32(&bm[(fm0 + o) % NM]), ((fm0 + o) / NM) & 1);
+      }
+      if (!ok) {
+        s_bad = 1;
+        atomicExch(err, 1);
+      }
+      __syncthreads();
+      if (s_bad) return false;
+      const S *tq = (const S *)(smem + ((fw0 + n) % NW) * G::W_BYTES);
+#pragma unroll
+      for (int v = 0; v < 9; ++v) win[v][P0] = ld2(tq + (v * BY + ys) * BX + xs);
+      if (o >= 0) {
+        const int k = q0 + n * DIR - DIR;
+        const S *xy = (const S *)(smem + ((fw0 + n + NW - 1) % NW) * G::W_BYTES);  // plane k
+        const S *cf = (const S *)(smem + G::OFF_C + ((fc0 + o) % NC) * G::C_BYTES);
+        float2 mx[3], my[3], mz[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          mx[q] = ld2(cf + q * PLANE + cidx);
+          my[q] = ld2(cf + (3 + q) * PLANE + cidx);
+          mz[q] = ld2(cf + (6 + q) * PLANE + cidx);
+        }
+        const float2 mu = ld2(cf + 9 * PLANE + cidx), lam = ld2(cf + 10 * PLANE + cidx);
+        const float2 bu = f2mul(ld2(cf + 11 * PLANE + cidx), pk((float)CRHO_OF<S>::v));
+        const float2 bzd = pk(__ldg(pz + L.nz_ + k) * DT * gz);
+        float2 h[9], Lr[9];
+        ElasticSum2 es;
+        // x direction: taps of the pair from the plane's row; the centre
+        // pair (plane k at i, i + 1) is window slot P1
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+          const S *row = xy + (v * BY + ys) * BX + xs;
+          const float2 cen = win[v][P1];
+          if (FB1 > 0) {
+            const float xm1 = ldv(row - 1), x4 = ldv(row + 4);
+            const float2 w23 = ld2(row + 2);
+            Lr[v] = stencil2(make_float2(xm1, cen.x), cen, make_float2(cen.y, w23.x), w23,
+                             make_float2(w23.y, x4));
+          } else {
+            const float xm3 = ldv(row - 3), x2 = ldv(row + 2);
+            const float2 w21 = ld2(row - 2);
+            Lr[v] = stencil2(make_float2(cen.y, x2), cen, make_float2(w21.y, cen.x), w21,
+                             make_float2(xm3, w21.x));
+          }
+        }
+        es.add<true>(mx, bxd, Lr);
+        // y direction
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+          const S *c0 = xy + (v * BY + ys) * BX + xs;
+          Lr[v] = stencil2(ld2(c0 - FB2 * BX), win[v][P1], ld2(c0 + FB2 * BX),
+                           ld2(c0 + 2 * FB2 * BX), ld2(c0 + 3 * FB2 * BX));
+        }
+        es.add<false>(my, byd, Lr);
+        // z direction: W[k - m*DIR] for m = -1..3 sits in slots P0 (q = k + DIR) .. P4
+#pragma unroll
+        for (int v = 0; v < 9; ++v)
+          Lr[v] = stencil2(win[v][P0], win[v][P1], win[v][P2], win[v][P3], win[v][P4]);
+        es.add<false>(mz, bzd, Lr);
+        es.finish(mu, lam, bu, h);
+        // RK4 combination (wave_rk.cpp:13-99), as the one-point kernel
+        const S *ms = (const S *)(smem + G::OFF_M + ((fm0 + o) % NM) * G::M_BYTES);
+        const S *ts = ms + 9 * PLANE;
+        const long long ctr = L.at(i, j, k);
+        const float cT = RK == 0 ? kB1 : RK == 1 ? cB : 0.0f;
+        const float cO = RK == 0 ? kA2rk : RK == 1 ? cA : kB4;
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+          const long long q = ctr + v * fs;
+          float2 base_t, base_o;
+          if (RK == 0) {
+            base_t = base_o = win[v][P1];
+          } else if (RK == 1) {
+            base_t = ld2(ts + v * PLANE + cidx);
+            base_o = ld2(ms + v * PLANE + cidx);
+          } else {
+            base_t = pk(0.0f);
+            base_o = ld2(ts + v * PLANE + cidx);
+          }
+          st2(a.wout + q, f2fma(pk(cO), h[v], base_o));
+          if (RK <= 1) st2(a.t + q, f2fma(pk(cT), h[v], base_t));
+        }
+      }
+      __syncthreads();  // every thread is done with W plane n-1, C and M slot of o
+      if (tid == 0) {
+        if (n + NW - 1 < nplanes) issue_w(n + NW - 1);
+        if (o >= 0 && o + NC < nout) issue_c(o + NC);
+        if (o >= 0 && need_t && o + NM < nout) issue_m(o + NM);
+      }
+      return true;
+    };
+    int n = 0;
+    while (n < nplanes) {
+      if (!iter(std::integral_constant<int, 0>{}, n)) break;
+      if (++n >= nplanes) break;
+      if (!iter(std::integral_constant<int, 1>{}, n)) break;
+      if (++n >= nplanes) break;
+      if (!iter(std::integral_constant<int, 2>{}, n)) break;
+      if (++n >= nplanes) break;
+      if (!iter(std::integral_constant<int, 3>{}, n)) break;
+      if (++n >= nplanes) break;
+      if (!iter(std::integral_constant<int, 4>{}, n)) break;
+      ++n;
+    }
+    if (n < nplanes) {
+      // error exit: drain what was issued and not yet waited for (bounded)
+      if (tid == 0) {
+        for (int m = n + 1; m < nplanes && m < n + NW - 1; ++m)
+          mbar_wait_bounded(smem_u32(&bw[(fw0 + m) % NW]), ((fw0 + m) / NW) & 1);
+        const int o = n - 4 > 0 ? n - 4 : 0;
+        for (int m = o; m < nout && m < o + NC; ++m)
+          mbar_wait_bounded(smem_u32(&bc[(fc0 + m) % NC]), ((fc0 + m) / NC) & 1);
+        if (need_t)
+          for (int m = o; m < nout && m < o + NM; ++m)
+            mbar_wait_bounded(smem_u32(&bm[(fm0 + m) % NM]), ((fm0 + m) / NM) & 1);
+      }
+      break;
+    }
+    fw0 += nplanes;
+    fc0 += nout;
+    if (need_t) fm0 += nout;
+  }
+}
+
 // Sets a kernel's dynamic shared-memory limit once per device.  `done` is
 // the kernel variant's own bit set of devices that have it; the attribute
 // call is idempotent, so two host threads that race here both make it and
@@ -922,6 +1235,58 @@ cudaError_t launch_one(const StageArgs<S> &a, const Maps &maps, int *err, int *c
     if (nlaunch) ++*nlaunch;
   }
   return cudaSuccess;
+}
+
+// One stage with the paired-point kernel for the interior (64 x 8 tiles:
+// pairs of 32 x 8 tiles of the Work grid that touch no PML slab and lie
+// inside the grid) and the one-point 32 x 8 PML variant for every other
+// tile and chunk (an odd interior tile column and partial edge tiles
+// included).  16-bit storage only.
+template <typename S, int FB1, int FB2, int FB3, int RK>
+cudaError_t launch_one_pair(const StageArgs<S> &a, const Maps &m8, const Maps &mp, int *err,
+                            int *counter, cudaStream_t st, int *nlaunch) {
+  if constexpr (sizeof(S) != 2) {
+    return cudaErrorInvalidValue;
+  } else {
+    const int nsm = sm_count();
+    WorkPlan wp = plan_work<S, 8>(a, nsm, counter);
+    Work w = wp.wk;
+    const int nx = a.L.nx_ - 2 * HALO, ny = a.L.ny_ - 2 * HALO;
+    // full tiles only, an even number of them in x
+    int bx_hi = std::min(w.bx_hi, nx / TX), by_hi = std::min(w.by_hi, ny / 8);
+    if (bx_hi - w.bx_lo < 2 || by_hi <= w.by_lo) {
+      bx_hi = w.bx_lo;
+      by_hi = w.by_lo;
+    }
+    bx_hi = w.bx_lo + (bx_hi - w.bx_lo) / 2 * 2;
+    w.bx_hi = bx_hi;
+    w.by_hi = by_hi;
+    const int tiles = w.ntx * w.nty, tiles_in = (w.bx_hi - w.bx_lo) * (w.by_hi - w.by_lo);
+    cudaError_t e = cudaSuccess;
+    Work wi = w;
+    wi.nitems = tiles_in / 2 * w.nic;
+    if (wi.nitems > 0) {
+      using G = PairGeo<S>;
+      static std::atomic<unsigned long long> attr_done{0};
+      auto kern = stage_pair_kernel<S, FB1, FB2, FB3, RK>;
+      e = ensure_smem_attr(kern, G::SMEM, attr_done);
+      if (e != cudaSuccess) return e;
+      e = cudaMemsetAsync(wi.counter, 0, sizeof(int), st);
+      if (e != cudaSuccess) return e;
+      kern<<<std::min(wi.nitems, nsm), G::NTHR, G::SMEM, st>>>(mp, a, wi, err);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+      if (nlaunch) ++*nlaunch;
+    }
+    Work wq = w;
+    wq.nitems = w.nzc * tiles + (tiles - tiles_in) * w.nic;
+    if (wq.nitems > 0) {
+      e = launch_variant<S, 8, FB1, FB2, FB3, true, RK>(a, m8, wq, err, nsm, st);
+      if (e != cudaSuccess) return e;
+      if (nlaunch) ++*nlaunch;
+    }
+    return cudaSuccess;
+  }
 }
 
 template <typename S, int FB1, int FB2, int FB3, bool PMLK, int RK>
@@ -1056,6 +1421,15 @@ int encode_stream_maps(const S *wave, const S *cjm, const S *wm, const S *t, con
     if (!rc) rc = encode_map<S>(wm, L, 9, TX, ty, 9, &m.m);
     if (!rc) rc = encode_map<S>(t, L, 9, TX, ty, 9, &m.t);
   }
+  if constexpr (sizeof(S) == 2) {  // the paired-point kernel's 64 x 8 tiles
+    using G = PairGeo<S>;
+    Maps &m = ms.pair;
+    if (!rc) rc = encode_map<S>(wave, L, 9, G::BX, G::BY, 9, &m.w);
+    if (!rc) rc = encode_map<S>(cjm, L, 13, G::TXP, G::TY, 9, &m.c9);
+    if (!rc) rc = encode_map<S>(cjm, L, 13, G::TXP, G::TY, 3, &m.c3);
+    if (!rc) rc = encode_map<S>(wm, L, 9, G::TXP, G::TY, 9, &m.m);
+    if (!rc) rc = encode_map<S>(t, L, 9, G::TXP, G::TY, 9, &m.t);
+  }
   if (!rc) std::memcpy(out, &ms, sizeof ms);
   return rc;
 }
@@ -1078,6 +1452,31 @@ cudaError_t launch_fb_rk(const StageArgs<S> &a, const Maps &m, int *err, int *co
     default: return launch_one<S, TYv, 1, 1, 1, RK>(a, m, err, counter, st, nlaunch);
   }
 }
+template <typename S, int RK>
+cudaError_t launch_fb_rk_pair(const StageArgs<S> &a, const MapSet &ms, int *err, int *counter,
+                              cudaStream_t st, int *nlaunch) {
+  const Maps &m8 = ms.ty8, &mp = ms.pair;
+  switch ((a.fb1 > 0) * 4 + (a.fb2 > 0) * 2 + (a.fb3 > 0)) {
+    case 0: return launch_one_pair<S, -1, -1, -1, RK>(a, m8, mp, err, counter, st, nlaunch);
+    case 1: return launch_one_pair<S, -1, -1, 1, RK>(a, m8, mp, err, counter, st, nlaunch);
+    case 2: return launch_one_pair<S, -1, 1, -1, RK>(a, m8, mp, err, counter, st, nlaunch);
+    case 3: return launch_one_pair<S, -1, 1, 1, RK>(a, m8, mp, err, counter, st, nlaunch);
+    case 4: return launch_one_pair<S, 1, -1, -1, RK>(a, m8, mp, err, counter, st, nlaunch);
+    case 5: return launch_one_pair<S, 1, -1, 1, RK>(a, m8, mp, err, counter, st, nlaunch);
+    case 6: return launch_one_pair<S, 1, 1, -1, RK>(a, m8, mp, err, counter, st, nlaunch);
+    default: return launch_one_pair<S, 1, 1, 1, RK>(a, m8, mp, err, counter, st, nlaunch);
+  }
+}
+template <typename S>
+cudaError_t launch_pair(const StageArgs<S> &a, const MapSet &ms, int *err, int *counter,
+                        cudaStream_t st, int *nlaunch) {
+  switch (rk_class(a.irk)) {
+    case 0: return launch_fb_rk_pair<S, 0>(a, ms, err, counter, st, nlaunch);
+    case 1: return launch_fb_rk_pair<S, 1>(a, ms, err, counter, st, nlaunch);
+    default: return launch_fb_rk_pair<S, 3>(a, ms, err, counter, st, nlaunch);
+  }
+}
+
 template <typename S, int TYv>
 cudaError_t launch_fb(const StageArgs<S> &a, const Maps &m, int *err, int *counter,
                       cudaStream_t st, int *nlaunch) {
@@ -1112,9 +1511,16 @@ cudaError_t launch_stage_stream(const StageArgs<S> &a, const void *maps_in, int 
   const MapSet &ms = *(const MapSet *)maps_in;
   // tile height 16 runs the batched kernel as a batch of one, so that a
   // scenario gives the same bits alone and inside a batch
-  cudaError_t e = tile_rows == 8
-                      ? launch_fb<S, 8>(a, ms.ty8, err, counter, st, nlaunch)
-                      : launch_stage_stream_batch<S>(&a, &maps_in, 1, err, counter, st, nlaunch);
+  cudaError_t e;
+  if (tile_rows == kTilePair) {
+    if constexpr (sizeof(S) == 2)
+      e = launch_pair<S>(a, ms, err, counter, st, nlaunch);
+    else
+      e = cudaErrorInvalidValue;
+  } else {
+    e = tile_rows == 8 ? launch_fb<S, 8>(a, ms.ty8, err, counter, st, nlaunch)
+                       : launch_stage_stream_batch<S>(&a, &maps_in, 1, err, counter, st, nlaunch);
+  }
   if (e != cudaSuccess) return e;
   if (after_main) e = cudaEventRecord(after_main, st);
   return e;

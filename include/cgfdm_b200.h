@@ -174,11 +174,15 @@ int cgfdm_get_timing(cgfdm_handle *h, float *ms3);
  * ms, [6] stages timed, [7] the streaming kernel's tile height (0: not used). */
 int cgfdm_get_kernel_stats(cgfdm_handle *h, double *out8);
 
-/* Tile height of the streaming kernel: 16 (32 x 16 tiles, one CTA per SM),
- * 8 (32 x 8 tiles, two CTAs per SM), or 0 (the default): autotune -- the
- * first cgfdm_run times one stage with each height on this handle's buffers
- * (blocking that call for a few stage times) and keeps the fastest; the
- * choice is cached per (precision, grid) for the process. */
+/* Tile form of the streaming kernel: 16 (32 x 16 tiles, one CTA per SM),
+ * 8 (32 x 8 tiles, two CTAs per SM), 64 (FP16 / BF16 storage only: 64 x 8
+ * interior tiles with two x-adjacent points per thread, the 32 x 8 form
+ * elsewhere), or 0 (the default): autotune -- the first cgfdm_run times one
+ * stage with each form on this handle's buffers (blocking that call for a
+ * few stage times) and keeps the fastest; the choice is cached per
+ * (precision, grid) for the process.  The forms split the grid differently
+ * between the interior launch and the PML launch, whose variants round the
+ * elastic combination differently, so they agree to rounding. */
 int cgfdm_set_tile_rows(cgfdm_handle *h, int32_t rows);
 
 /* Checkpoint / resume at a step boundary (no counterpart in the reference):

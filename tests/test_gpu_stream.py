@@ -133,3 +133,72 @@ def test_stream_matches_exact_on_tiny_and_ragged_grids(gpu_available, shape, row
     assert np.isfinite(s[1]).all()
     assert rel_l2(s[1], e[1]) < 1e-5
     assert rel_l2(s[0], e[0]) < 1e-5
+
+
+FORM_SHAPES = [(200, 60, 40, 6), (150, 45, 30, 0), (131, 83, 37, 9)]
+
+
+def _run_form(sc, prec, form, steps=12):
+    nx, ny, nz, npml = sc["dims"]
+    d = cgfdm.make_desc(nx, ny, nz, npml, 100.0, 0.008, steps, prec, cgfdm.KERNEL_STREAM)
+    with cgfdm.Simulation(d) as sim:
+        sim.set_tile_rows(form)
+        sim.set_model(sc["cjm"], sc["rdz"])
+        sim.set_point_source(*sc["src"], 6.0)
+        sim.set_stations(sc["sta"])
+        sim.run(steps)
+        assert sim.kernel_stats()["tile_rows"] == form
+        return sim.wavefield(), sim.stations(), sim.pgv()
+
+
+def _case(shape, precision):
+    from test_gpu_batch import _scaled, _synthetic
+    nx, ny, nz, npml = shape
+    sc = _synthetic(nx, ny, nz, npml, seed=nx + ny)
+    prec = {"fp32": cgfdm.FP32, "fp16": cgfdm.FP16, "bf16": cgfdm.BF16}[precision]
+    return (sc if precision == "fp32" else _scaled(sc)), prec
+
+
+@pytest.mark.parametrize("precision", ["fp16", "bf16"])
+@pytest.mark.parametrize("shape", [(168, 60, 40, 6), (128, 48, 30, 0)])
+def test_paired_form_is_bitwise_the_one_point_kernel(gpu_available, precision, shape):
+    """The paired-point kernel (64 x 8 tiles, two points per thread) computes
+    each point with the one-point kernel's operations in the same order: on
+    grids where both forms give the same points to the interior launch (an
+    even number of interior 32-column tiles, full tiles), the paired form
+    and the 32 x 8 form give bit-identical wavefields, seismograms and PGV
+    over 12 steps (every RK stage and MacCormack sign triple)."""
+    sc, prec = _case(shape, precision)
+    ref = _run_form(sc, prec, 8)
+    got = _run_form(sc, prec, 64)
+    assert np.isfinite(ref[0]).all() and np.abs(ref[0]).max() > 0
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b), rel_l2(a, b)
+
+
+@pytest.mark.parametrize("precision", ["fp16", "bf16", "fp32"])
+@pytest.mark.parametrize("shape", FORM_SHAPES)
+def test_tile_forms_agree(gpu_available, precision, shape):
+    """All tile forms (32 x 16, 32 x 8, and for 16-bit storage the paired
+    64 x 8 form) over 12 steps on grids with an odd number of interior
+    32-column tiles, partial edge tiles and no PML.  The forms split the
+    grid differently between the interior and PML launches, whose variants
+    round the elastic combination differently, so they agree to rounding:
+    relative L2 <= 1e-6 (FP32) or 1e-3 (16-bit storage)."""
+    sc, prec = _case(shape, precision)
+    forms = [16, 8] + ([64] if precision != "fp32" else [])
+    out = {form: _run_form(sc, prec, form) for form in forms}
+    ref = out[8]
+    assert np.isfinite(ref[0]).all() and np.abs(ref[0]).max() > 0
+    tol = 1e-6 if precision == "fp32" else 1e-3
+    for form in forms:
+        for a, b in zip(out[form], ref):
+            assert np.isfinite(a).all()
+            assert rel_l2(a, b) <= tol, (form, rel_l2(a, b))
+
+
+def test_paired_form_is_refused_for_fp32(gpu_available):
+    d = cgfdm.make_desc(40, 30, 20, 4, 100.0, 0.008, 2, cgfdm.FP32, cgfdm.KERNEL_STREAM)
+    with cgfdm.Simulation(d) as sim:
+        with pytest.raises(Exception):
+            sim.set_tile_rows(64)
