@@ -475,6 +475,8 @@ def main():
                     help="streaming-kernel tile form: 16 or 8 (32-column tiles of that height), "
                          "64 (paired-point 64 x 8 tiles, FP16 / BF16), 0: the library's "
                          "autotuner")
+    ap.add_argument("--chunk", type=int, default=0,
+                    help="planes per streaming work item in z (0: the library's default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp16", action="store_true",
                     help="skip the scaled-FP16 companion measurement of an FP32 run")
@@ -572,6 +574,7 @@ def main():
                                prec, kern, local)
         sim = cgfdm.Simulation(desc)
         sim.set_tile_rows(args.tile_rows)
+        sim.set_chunk(args.chunk)
         sim.set_model(cjm, setup["rdz"])
         if setup["point"] is not None:
             sim.set_point_source(*setup["point"], setup["rickerfc"])
@@ -603,6 +606,7 @@ def main():
     ms = ev0.elapsed_time(ev1)
     tm = sim.timing_ms()
     ks = sim.kernel_stats()
+    form, chunk = sim.tuning()
     stage_ms, stage_n = float(tm[1]), int(tm[2])
     sim.close()
     value, ms_max = replica_throughput(torch, dist, ms / 1e3, npts, args.steps, ws, "cuda")
@@ -653,6 +657,7 @@ def main():
         sim16 = cgfdm.Simulation(cgfdm.make_desc(e0.nx, e0.ny, e0.nz, e0.npml, e0.dh, e0.dt,
                                                  total_steps, cgfdm.FP16, kern, local))
         sim16.set_tile_rows(args.tile_rows)
+        sim16.set_chunk(args.chunk)
         sim16.set_model(s16["cjm"], s16["rdz"])
         if s16["point"] is not None:
             sim16.set_point_source(*s16["point"], s16["rickerfc"])
@@ -671,10 +676,11 @@ def main():
         torch.cuda.synchronize()
         ms16 = ev0.elapsed_time(ev1)
         ks16 = sim16.kernel_stats()
+        form16, chunk16 = sim16.tuning()
         sim16.close()
         v16, ms16_max = replica_throughput(torch, dist, ms16 / 1e3, npts, args.steps, ws, "cuda")
         fp16 = {"value": v16, "unit": UNIT, "ms_per_step": ms16_max * 1e3 / args.steps,
-                "speedup_vs_fp32": v16 / value, "tile_rows": ks16["tile_rows"],
+                "speedup_vs_fp32": v16 / value, "tile_form": form16, "chunk_planes": chunk16,
                 "bytes_per_point_step": BYTES_PER_POINT_STEP["fp16"]}
 
     # error against FP64 of the precisions of this line, measured in this run
@@ -704,7 +710,8 @@ def main():
     # when the precision has no streaming form)
     if ks["stream_launches"] > 0 and ks["stream_ms"] > 0:
         # tile height 16 runs the batched form of the kernel (a batch of one)
-        kname = "stage_stream_batch_kernel" if ks["tile_rows"] == 16 else "stage_stream_kernel"
+        kname = {16: "stage_stream_batch_kernel", 8: "stage_stream_kernel",
+                 64: "stage_pair_kernel"}.get(form, "stage_stream_kernel")
         kms, klaunch = ks["stream_ms"], ks["stream_launches"]
         kbytes = ks["stream_bytes"]
     else:
@@ -754,7 +761,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": w["name"], "precision": args.precision,
                        "grid": [desc0.nx, desc0.ny, desc0.nz], "points": npts,
-                       "kernel": args.kernel, "tile_rows": ks["tile_rows"],
+                       "kernel": args.kernel, "tile_form": form, "chunk_planes": chunk,
                        "parallelism": "replicas" if ws > 1 else "single",
                        "l2": "inputs larger than L2 (%.2f GB per wavefield buffer), no flush" % (
                            9 * (desc0.nx + 6) * (desc0.ny + 6) * (desc0.nz + 6) *

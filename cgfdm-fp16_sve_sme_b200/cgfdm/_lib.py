@@ -88,6 +88,8 @@ SIGNATURES = {
     "cgfdm_get_timing": (C.c_int, [P, P]),
     "cgfdm_get_kernel_stats": (C.c_int, [P, P]),
     "cgfdm_set_tile_rows": (C.c_int, [P, I32]),
+    "cgfdm_set_chunk": (C.c_int, [P, I32]),
+    "cgfdm_get_tuning": (C.c_int, [P, P]),
     "cgfdm_set_graph": (C.c_int, [P, I32]),
     "cgfdm_inject_fault": (C.c_int, [P, I32]),
     "cgfdm_checkpoint_bytes": (C.c_int, [P, C.POINTER(I64)]),

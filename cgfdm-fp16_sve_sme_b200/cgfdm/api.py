@@ -131,6 +131,16 @@ class Simulation:
         """Replay each step of run() as a CUDA graph (results are identical)."""
         check(lib().cgfdm_set_graph(self._h, int(on)))
 
+    def set_chunk(self, planes):
+        """Planes per streaming work item in z (0: automatic)."""
+        check(lib().cgfdm_set_chunk(self._h, int(planes)))
+
+    def tuning(self):
+        """(tile form, planes per work item) of the streaming kernel."""
+        v = np.zeros(2, np.int32)
+        check(lib().cgfdm_get_tuning(self._h, _ptr(v)))
+        return int(v[0]), int(v[1])
+
     def set_tile_rows(self, rows):
         """Streaming-kernel tile height: 16, 8, or 0 to autotune at the first run."""
         check(lib().cgfdm_set_tile_rows(self._h, int(rows)))

@@ -256,9 +256,23 @@ int cgfdm_batch_destroy(cgfdm_batch *b) {
   return CGFDM_OK;
 }
 
+int cgfdm_set_chunk(cgfdm_handle *h, int32_t planes) {
+  H_OR_FAIL(h);
+  return h->eng->set_chunk(planes);
+}
+
 int cgfdm_set_tile_rows(cgfdm_handle *h, int32_t rows) {
   H_OR_FAIL(h);
   return h->eng->set_tile_rows(rows);
+}
+
+int cgfdm_get_tuning(cgfdm_handle *h, int32_t *form_chunk) {
+  H_OR_FAIL(h);
+  if (!form_chunk) {
+    set_error("null output");
+    return CGFDM_ERR_ARG;
+  }
+  return h->eng->get_tuning(form_chunk);
 }
 
 int cgfdm_get_kernel_stats(cgfdm_handle *h, double *out8) {

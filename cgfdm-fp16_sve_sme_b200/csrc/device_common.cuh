@@ -106,6 +106,9 @@ template <typename S> struct StageArgs {
   int npml;
   float rDH, DT;
   int fb1, fb2, fb3, irk;
+  // planes per upper z chunk of the streaming kernel's work items (0: about
+  // 40 items per CTA slot, chunks of at least 16 planes)
+  int chunk;
   // failure-detection tests only: the streaming kernel leaves one input-plane
   // load of its first work item unissued, so that the bounded wait on it
   // expires (no memory is touched); 0 in every normal launch

@@ -55,7 +55,9 @@ const int kFB[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1},  {-1, -1, 1},
 // Autotuner results: streaming-kernel tile height per (precision, nx, ny, nz,
 // nPML), shared by every handle of the process.
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int>, int> g_tuned;
+// autotuned (tile form, work-item depth) per (precision, nx, ny, nz, nPML,
+// fixed depth or -1)
+std::map<std::tuple<int, int, int, int, int, int>, std::pair<int, int>> g_tuned;
 
 struct Dims {
   int nx, ny, nz, npml;
@@ -644,6 +646,17 @@ template <typename S> class EngineT : public Engine {
     return CGFDM_OK;
   }
 
+  int set_chunk(int planes) override {
+    if (planes < 0) {
+      set_error("chunk must be 0 (automatic) or a positive number of planes");
+      return CGFDM_ERR_ARG;
+    }
+    chunk_ = planes;
+    chunk_fixed_ = planes > 0;
+    drop_graphs();
+    return CGFDM_OK;
+  }
+
   int set_graph(bool on) override {
     use_graph_ = on;
     drop_graphs();
@@ -693,6 +706,12 @@ template <typename S> class EngineT : public Engine {
     return CGFDM_OK;
   }
 
+  int get_tuning(int32_t *form_chunk) override {
+    form_chunk[0] = use_stream_ ? (tile_rows_ ? tile_rows_ : 16) : 0;
+    form_chunk[1] = use_stream_ ? chunk_ : 0;
+    return CGFDM_OK;
+  }
+
   const cgfdm_desc &desc() const override { return d_; }
 
  private:
@@ -737,6 +756,7 @@ template <typename S> class EngineT : public Engine {
     a.DT = d_.dt;
     a.fb1 = fb[0]; a.fb2 = fb[1]; a.fb3 = fb[2];
     a.irk = irk;
+    a.chunk = chunk_;
     a.nslab = g_.npml > 0 ? 5 : 0;
     size_t off = 0;
     for (int s = 0; s < a.nslab; ++s) {
@@ -754,56 +774,74 @@ template <typename S> class EngineT : public Engine {
     return a;
   }
 
-  // Picks the streaming kernel's tile form for this grid and precision (32 x
-  // 16, 32 x 8, and for 16-bit storage the paired-point 64 x 8 form):
-  // times stage 0 at the current step boundary with each candidate (stage 0
-  // reads only the step state and writes buffers the next stage 0 rewrites)
-  // and keeps the fastest; results are cached per (precision, grid).
+  // Picks the streaming kernel's tile form (32 x 16, 32 x 8, and for 16-bit
+  // storage the paired-point 64 x 8 form) and work-item depth in z (automatic,
+  // 64 or 32 planes; the depth set by cgfdm_set_chunk is kept) for this grid
+  // and precision: times the streaming part of stages 0 and 1 at the current
+  // step boundary with each candidate and keeps the fastest.  Stage 0 reads
+  // only the step state A and step-start auxiliaries and writes X, T and the
+  // stage-1 auxiliary inputs; stage 1 reads those and writes Y and T; the
+  // real step rewrites all of them before reading them, so the timing leaves
+  // the run unchanged.  Results are cached per (precision, grid).
   int tune(cudaStream_t st) {
-    const auto key = std::make_tuple((int)d_.precision, d_.nx, d_.ny, d_.nz, d_.npml);
+    const auto key = std::make_tuple((int)d_.precision, d_.nx, d_.ny, d_.nz, d_.npml,
+                                     chunk_fixed_ ? chunk_ : -1);
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
       auto f = g_tuned.find(key);
       if (f != g_tuned.end()) {
-        tile_rows_ = f->second;
+        tile_rows_ = f->second.first;
+        chunk_ = f->second.second;
         return CGFDM_OK;
       }
     }
-    const int fb[3] = {kFB[it_ % 8][0], kFB[it_ % 8][1], kFB[it_ % 8][2]};
-    StageArgs<S> b = stage_args(0, fb);
-    b.kbeg = HALO;
-    b.kend = g_.L.nz_ - HALO - 3;
+    const int fb0[3] = {kFB[it_ % 8][0], kFB[it_ % 8][1], kFB[it_ % 8][2]};
+    const int fb1[3] = {-fb0[0], -fb0[1], -fb0[2]};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
-    int best = 16;
-    float best_ms = 1e30f;
-    cudaError_t err = cudaSuccess;
     std::vector<int> forms = {16, 8};
     if (sizeof(S) == 2) forms.push_back(kTilePair);
-    for (int rows : forms) {
-      err = launch_stage_stream<S>(b, tmap_[0], err_flag_, err_flag_ + 1, st, nullptr, nullptr,
-                                   rows);
-      if (err == cudaSuccess) err = cudaEventRecord(e0, st);
-      for (int r = 0; r < 2 && err == cudaSuccess; ++r)
-        err = launch_stage_stream<S>(b, tmap_[0], err_flag_, err_flag_ + 1, st, nullptr,
-                                     nullptr, rows);
-      if (err == cudaSuccess) err = cudaEventRecord(e1, st);
-      if (err == cudaSuccess) err = cudaEventSynchronize(e1);
-      float ms = 0;
-      if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
-      if (err != cudaSuccess) break;
-      if (ms < best_ms) {
-        best_ms = ms;
-        best = rows;
+    std::vector<int> chunks = {0, 64, 32};
+    if (chunk_fixed_) chunks = {chunk_};
+    int best_form = 16, best_chunk = chunks[0];
+    float best_ms = 1e30f;
+    cudaError_t err = cudaSuccess;
+    for (int rows : forms)
+      for (int ch : chunks) {
+        StageArgs<S> b0 = stage_args(0, fb0), b1 = stage_args(1, fb1);
+        b0.kbeg = b1.kbeg = HALO;
+        b0.kend = b1.kend = g_.L.nz_ - HALO - 3;
+        b0.chunk = b1.chunk = ch;
+        auto pair = [&]() {
+          cudaError_t e = launch_stage_stream<S>(b0, tmap_[0], err_flag_, err_flag_ + 1, st,
+                                                 nullptr, nullptr, rows);
+          if (e == cudaSuccess)
+            e = launch_stage_stream<S>(b1, tmap_[1], err_flag_, err_flag_ + 1, st, nullptr,
+                                       nullptr, rows);
+          return e;
+        };
+        err = pair();
+        if (err == cudaSuccess) err = cudaEventRecord(e0, st);
+        for (int r = 0; r < 2 && err == cudaSuccess; ++r) err = pair();
+        if (err == cudaSuccess) err = cudaEventRecord(e1, st);
+        if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+        float ms = 0;
+        if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+        if (err != cudaSuccess) break;
+        if (ms < best_ms) {
+          best_ms = ms;
+          best_form = rows;
+          best_chunk = ch;
+        }
       }
-    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     CUDA_TRY(err);
-    tile_rows_ = best;
+    tile_rows_ = best_form;
+    chunk_ = best_chunk;
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tuned[key] = best;
+    g_tuned[key] = {best_form, best_chunk};
     return CGFDM_OK;
   }
 
@@ -981,6 +1019,8 @@ template <typename S> class EngineT : public Engine {
   int stage_used_ = 0;
   int launches_ = 0;          // kernels launched by the last run()
   int tile_rows_ = 0;         // streaming-kernel tile height; 0 = autotune at the first run()
+  int chunk_ = 0;             // planes per streaming work item in z; 0 = automatic
+  bool chunk_fixed_ = false;  // set by set_chunk: the autotuner keeps chunk_
   bool drop_next_load_ = false;  // fault injection for failure-detection tests
   int *step_ = nullptr;       // device copy of it_
   float *moment_tab_ = nullptr;            // point-source moment per step

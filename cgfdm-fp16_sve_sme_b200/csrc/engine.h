@@ -44,7 +44,9 @@ class Engine {
   virtual int set_timing(bool on) = 0;
   virtual int get_timing(float *ms3) = 0;
   virtual int get_kernel_stats(double *out8) = 0;
+  virtual int get_tuning(int32_t *form_chunk) = 0;
   virtual int set_tile_rows(int rows) = 0;
+  virtual int set_chunk(int planes) = 0;
   virtual int set_graph(bool on) = 0;
   virtual int inject_fault(int kind) = 0;
   virtual int64_t checkpoint_bytes() const = 0;

@@ -552,12 +552,17 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
     for (int v = 0; v < 9; ++v)
 #pragma unroll
       for (int m = 0; m < 5; ++m) win[v][m] = 0.0f;
+    // z-profile beta of the next output plane, loaded one iteration ahead
+    // (its latency then overlaps the barrier and ring waits)
+    float bz_next = 0.0f;
 
     // one input plane with window rotation R = n mod 5; false on a failed wait
     auto iter = [&](auto Rc, const int n) -> bool {
       constexpr int R = decltype(Rc)::value;
       constexpr int P0 = R, P1 = (R + 4) % 5, P2 = (R + 3) % 5, P3 = (R + 2) % 5, P4 = (R + 1) % 5;
       const int o = n - 4;  // output index of this iteration (o < 0: window warm-up)
+      const float bz_cur = bz_next;
+      if (o + 1 >= 0 && n + 1 < nplanes) bz_next = __ldg(pz + L.nz_ + q0 + n * DIR);
       constexpr int HP = hoist_parts<RK>();
       // the inputs of this plane's point in its first slab (x, y or the
       // bottom z slab), issued before the waits
@@ -577,13 +582,15 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         ok = ok && mbar_wait_bounded(smem_u32(&bc[(fc0 + o) % NC]), ((fc0 + o) / NC) & 1);
         if (need_t) ok = ok && mbar_wait_bounded(smem_u32(&bm[(fm0 + o) % NM]), ((fm0 + o) / NM) & 1);
       }
+      // Every thread waits on the ring barriers itself, so no block barrier is
+      // needed before the plane is read; a thread whose wait expired skips the
+      // plane, and all threads leave after the barrier below.
       if (!ok) {
         s_bad = 1;
         atomicExch(err, 1);
       }
-      __syncthreads();
-      if (s_bad) return false;
       const S *tq = (const S *)(smem + ((fw0 + n) % NW) * G::W_BYTES);
+      if (ok) {
       if constexpr (G::CONV) {  // plane n to FP32 for the stencils of the next iteration
         constexpr int NE = 9 * BY * BX;
         static_assert(NE % 4 == 0, "conversion in groups of four");
@@ -615,7 +622,7 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         }
         const float mu = ldv(cf + 9 * NTHR + cidx), lam = ldv(cf + 10 * NTHR + cidx);
         const float bu = ldv(cf + 11 * NTHR + cidx) * (float)CRHO_OF<S>::v;
-        const float bzd = __ldg(pz + L.nz_ + k) * DT * gz;
+        const float bzd = bz_cur * DT * gz;
         float h[9], Lr[9], E[9];
         ElasticSum es;
         // Fields are taken in pairs (0,1) (2,3) (4,5) (6,7) and 8 for the
@@ -744,7 +751,9 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
           }
         }
       }
+      }  // ok
       __syncthreads();  // every thread is done with W plane n-1, C and M slot of o
+      if (s_bad) return false;
       if (tid == 0) {
         if (n + NW - 1 < nplanes) issue_w(n + NW - 1);
         if (o >= 0 && o + NC < nout) issue_c(o + NC);
@@ -826,7 +835,10 @@ __global__ void __launch_bounds__(TX * 16, 1)
 // operation order, rounding) is that of the one-point kernel's interior
 // variant, so both give the same bits.  Rings: W 4 slots (9 fields x 12 rows
 // x 80 columns: the tile, a 16-byte aligned 8-column halo on each side and
-// the y halo), coefficients 3 slots, m / t 3 slots; one CTA per SM.
+// the y halo), coefficients 3 slots, m / t 3 slots; one CTA per SM.  (An FP32
+// copy of each plane, converted once cooperatively, measured slower: the
+// extra barrier-bound work per plane and the shallower W ring cost more
+// than the conversions it saves.)
 template <typename S> struct PairGeo {
   static constexpr int TY = 8, TXP = 64, NTHR = 256, PLANE = TY * TXP;
   static constexpr int BY = TY + 4, BX = 8 + TXP + 8;
@@ -904,7 +916,7 @@ __global__ void __launch_bounds__(256, 1)
     stage_pair_kernel(const __grid_constant__ Maps maps, const __grid_constant__ StageArgs<S> a,
                       const __grid_constant__ Work wk, int *err) {
   using G = PairGeo<S>;
-  constexpr int TY = G::TY, PLANE = G::PLANE, BY = G::BY, BX = G::BX;
+  constexpr int TY = G::TY, PLANE = G::PLANE, BY = G::BY, BX = G::BX, NTHR = G::NTHR;
   constexpr int NW = G::NW, NC = G::NC, NM = G::NM;
   constexpr int DIR = -FB3;  // sweep direction in z
   extern __shared__ unsigned char smem_raw[];
@@ -993,26 +1005,32 @@ __global__ void __launch_bounds__(256, 1)
     for (int v = 0; v < 9; ++v)
 #pragma unroll
       for (int m = 0; m < 5; ++m) win[v][m] = pk(0.0f);
+    // z-profile beta of the next output plane, loaded one iteration ahead
+    // (its latency then overlaps the barrier and ring waits)
+    float bz_next = 0.0f;
 
     auto iter = [&](auto Rc, const int n) -> bool {
       constexpr int R = decltype(Rc)::value;
       constexpr int P0 = R, P1 = (R + 4) % 5, P2 = (R + 3) % 5, P3 = (R + 2) % 5, P4 = (R + 1) % 5;
       const int o = n - 4;
+      const float bz_cur = bz_next;
+      if (o + 1 >= 0 && n + 1 < nplanes) bz_next = __ldg(pz + L.nz_ + q0 + n * DIR);
       bool ok = mbar_wait_bounded(smem_u32(&bw[(fw0 + n) % NW]), ((fw0 + n) / NW) & 1);
       if (o >= 0) {
         ok = ok && mbar_wait_bounded(smem_u32(&bc[(fc0 + o) % NC]), ((fc0 + o) / NC) & 1);
         if (need_t) ok = ok && mbar_wait_bounded(smem_u32(&bm[(fm0 + o) % NM]), ((fm0 + o) / NM) & 1);
       }
+      // Every thread waits on the ring barriers itself, so no block barrier is
+      // needed before the plane is read; a thread whose wait expired skips the
+      // plane, and all threads leave after the barrier below.
       if (!ok) {
         s_bad = 1;
         atomicExch(err, 1);
       }
-      __syncthreads();
-      if (s_bad) return false;
       const S *tq = (const S *)(smem + ((fw0 + n) % NW) * G::W_BYTES);
 #pragma unroll
-      for (int v = 0; v < 9; ++v) win[v][P0] = ld2(tq + (v * BY + ys) * BX + xs);
-      if (o >= 0) {
+      for (int v = 0; v < 9; ++v) win[v][P0] = ok ? ld2(tq + (v * BY + ys) * BX + xs) : pk(0.0f);
+      if (o >= 0 && ok) {
         const int k = q0 + n * DIR - DIR;
         const S *xy = (const S *)(smem + ((fw0 + n + NW - 1) % NW) * G::W_BYTES);  // plane k
         const S *cf = (const S *)(smem + G::OFF_C + ((fc0 + o) % NC) * G::C_BYTES);
@@ -1025,7 +1043,7 @@ __global__ void __launch_bounds__(256, 1)
         }
         const float2 mu = ld2(cf + 9 * PLANE + cidx), lam = ld2(cf + 10 * PLANE + cidx);
         const float2 bu = f2mul(ld2(cf + 11 * PLANE + cidx), pk((float)CRHO_OF<S>::v));
-        const float2 bzd = pk(__ldg(pz + L.nz_ + k) * DT * gz);
+        const float2 bzd = pk(bz_cur * DT * gz);
         float2 h[9], Lr[9];
         ElasticSum2 es;
         // x direction: taps of the pair from the plane's row; the centre
@@ -1085,6 +1103,7 @@ __global__ void __launch_bounds__(256, 1)
         }
       }
       __syncthreads();  // every thread is done with W plane n-1, C and M slot of o
+      if (s_bad) return false;
       if (tid == 0) {
         if (n + NW - 1 < nplanes) issue_w(n + NW - 1);
         if (o >= 0 && o + NC < nout) issue_c(o + NC);
@@ -1203,9 +1222,11 @@ WorkPlan plan_work(const StageArgs<S> &a, int nsm, int *counter) {
   const int pl_p = wk.kz - a.kbeg, pl_i = a.kend - wk.kz;
   wk.nzc = pl_p > 0 ? (pl_p + 31) / 32 : 0;
   wk.chunk_p = wk.nzc ? (pl_p + wk.nzc - 1) / wk.nzc : 1;
-  // upper planes: about 40 items per CTA slot, chunks of at least 16 planes
+  // upper planes: a.chunk planes per item, or about 40 items per CTA slot
+  // with chunks of at least 16 planes
   int nic = pl_i > 0 ? (40 * nsm * slots + tiles - 1) / tiles : 0;
   if (pl_i > 0) nic = std::max(1, std::min(nic, pl_i / 16));
+  if (pl_i > 0 && a.chunk > 0) nic = (pl_i + a.chunk - 1) / a.chunk;
   wk.chunk_i = nic ? (pl_i + nic - 1) / nic : 1;
   wk.nic = nic ? (pl_i + wk.chunk_i - 1) / wk.chunk_i : 0;
   wk.nitems = 0;

@@ -185,6 +185,19 @@ int cgfdm_get_kernel_stats(cgfdm_handle *h, double *out8);
  * elastic combination differently, so they agree to rounding. */
 int cgfdm_set_tile_rows(cgfdm_handle *h, int32_t rows);
 
+/* Depth of the streaming kernel's work items: the planes above the bottom
+ * PML slab are cut into chunks of `planes` z planes per work item (0, the
+ * default: about 40 items per CTA slot, at least 16 planes each).  Shorter
+ * chunks keep neighbouring tiles closer in time (their halo rows meet in
+ * L2) but re-read four planes per chunk. */
+int cgfdm_set_chunk(cgfdm_handle *h, int32_t planes);
+
+/* The streaming kernel's tile form and work-item depth in use (after the
+ * autotuner, if it ran): form_chunk[0] = 16, 8 or 64, form_chunk[1] = planes
+ * per item (0: automatic); both 0 when the handle runs the exact-order
+ * kernel only. */
+int cgfdm_get_tuning(cgfdm_handle *h, int32_t *form_chunk);
+
 /* Checkpoint / resume at a step boundary (no counterpart in the reference):
  * the handle's raw device state -- step wavefield, the two other stage
  * buffers (their halo cells hold point-source values), step-start PML

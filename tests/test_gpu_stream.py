@@ -202,3 +202,34 @@ def test_paired_form_is_refused_for_fp32(gpu_available):
     with cgfdm.Simulation(d) as sim:
         with pytest.raises(Exception):
             sim.set_tile_rows(64)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+def test_work_item_depth_does_not_change_results(gpu_available, precision):
+    """The depth of the streaming work items in z (cgfdm_set_chunk) only
+    changes how the planes above the bottom PML slab are cut into items, not
+    how any point is computed: 0 (automatic), 32 and 7 planes give
+    bit-identical results; the autotuner's choice is reported."""
+    sc, prec = _case((131, 83, 37, 9), precision)
+    nx, ny, nz, npml = sc["dims"]
+    out = []
+    for chunk in (0, 32, 7):
+        d = cgfdm.make_desc(nx, ny, nz, npml, 100.0, 0.008, 12, prec, cgfdm.KERNEL_STREAM)
+        with cgfdm.Simulation(d) as sim:
+            sim.set_tile_rows(8)
+            sim.set_chunk(chunk)
+            sim.set_model(sc["cjm"], sc["rdz"])
+            sim.set_point_source(*sc["src"], 6.0)
+            sim.set_stations(sc["sta"])
+            sim.run(12)
+            assert sim.tuning() == (8, chunk)
+            out.append((sim.wavefield(), sim.stations()))
+    for a, b in zip(out[1:], [out[0]] * 2):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    # the autotuner picks a form and a depth among its candidates
+    d = cgfdm.make_desc(nx, ny, nz, npml, 100.0, 0.008, 2, prec, cgfdm.KERNEL_STREAM)
+    with cgfdm.Simulation(d) as sim:
+        sim.set_model(sc["cjm"], sc["rdz"])
+        sim.run(1)
+        form, chunk = sim.tuning()
+        assert form in ((16, 8, 64) if precision == "fp16" else (16, 8)) and chunk in (0, 64, 32)
