@@ -50,12 +50,15 @@ __global__ void fault_source_kernel(S *w, long long fs, const long long *idx, co
   }
 }
 
+// Stations and PGV of step *step, then the step counter advances: every
+// block reads *step first, and the last block to finish (counted in
+// step[1]) increments it, so the step ends with one launch.
 template <typename S>
 __global__ void station_pgv_kernel(const S *w, Layout L, const int *xyz, int nsta, int NT,
-                                   const int *step, float *wave, float *pgv, float c1, float c2,
+                                   int *step, float *wave, float *pgv, float c1, float c2,
                                    double cv_inv) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int it = *step;
+  const int it = *(volatile int *)step;
   const int nx = L.nx_ - 2 * HALO, ny = L.ny_ - 2 * HALO;
   if (t < nsta) {
     const long long c = L.at(xyz[3 * t], xyz[3 * t + 1], xyz[3 * t + 2]);
@@ -73,9 +76,16 @@ __global__ void station_pgv_kernel(const S *w, Layout L, const int *xyz, int nst
     if (pgv[2 * t] < vh) pgv[2 * t] = vh;
     if (pgv[2 * t + 1] < vv) pgv[2 * t + 1] = vv;
   }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(step + 1, 1) == (int)gridDim.x - 1) {
+      step[1] = 0;
+      step[0] = it + 1;
+      __threadfence();
+    }
+  }
 }
-
-__global__ void step_advance_kernel(int *step) { *step += 1; }
 
 template <typename S>
 __global__ void slice_pack_kernel(const S *f, Layout L, int axis, int at, double c, float *out) {
@@ -140,14 +150,9 @@ cudaError_t launch_fault_source(S *w, long long fs, const long long *idx, const 
   return cudaGetLastError();
 }
 
-cudaError_t launch_step_advance(int *step, cudaStream_t st) {
-  step_advance_kernel<<<1, 1, 0, st>>>(step);
-  return cudaGetLastError();
-}
-
 template <typename S>
 cudaError_t launch_station_pgv(const S *w, Layout L, const int *xyz, int nsta, int NT,
-                               const int *step, float *wave, float *pgv, float c1, float c2,
+                               int *step, float *wave, float *pgv, float c1, float c2,
                                double cv_inv, cudaStream_t st) {
   const int n = (L.nx_ - 2 * HALO) * (L.ny_ - 2 * HALO);
   const int total = n > nsta ? n : nsta;
@@ -183,8 +188,8 @@ cudaError_t launch_repack_out(const S *src, float *dst, Layout L, int nfield, cu
   template cudaError_t launch_fault_source<S>(S *, long long, const long long *, const float *,    \
                                               long long, const int *, const float *, const int *,  \
                                               float, cudaStream_t);                                \
-  template cudaError_t launch_station_pgv<S>(const S *, Layout, const int *, int, int,             \
-                                             const int *, float *, float *, float, float, double,  \
+  template cudaError_t launch_station_pgv<S>(const S *, Layout, const int *, int, int, int *,      \
+                                             float *, float *, float, float, double,               \
                                              cudaStream_t);                                        \
   template cudaError_t launch_slice_pack<S>(const S *, Layout, int, int, double, float *,         \
                                             cudaStream_t);                                         \

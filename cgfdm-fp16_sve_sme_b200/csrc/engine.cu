@@ -131,8 +131,8 @@ template <typename S> class EngineT : public Engine {
     CUDA_TRY(cudaMalloc(&err_flag_, 2 * sizeof(int)));
     CUDA_TRY(cudaMemsetAsync(err_flag_, 0, 2 * sizeof(int), own_stream_));
     // the device copy of the step counter it_ (read by the per-step kernels)
-    CUDA_TRY(cudaMalloc(&step_, sizeof(int)));
-    CUDA_TRY(cudaMemsetAsync(step_, 0, sizeof(int), own_stream_));
+    CUDA_TRY(cudaMalloc(&step_, 2 * sizeof(int)));  // the step, the end-of-step block counter
+    CUDA_TRY(cudaMemsetAsync(step_, 0, 2 * sizeof(int), own_stream_));
     for (int q = 0; q < 2; ++q) CUDA_TRY(cudaEventCreate(&ev_[q]));
     // opposite PML slabs that overlap (nPML above half the grid, a point in
     // both x1 and x2) are left to the exact-order kernel, which applies every
@@ -354,10 +354,10 @@ template <typename S> class EngineT : public Engine {
 
   int step_end(cudaStream_t st) {
     const float c1 = (float)(1.0 / SCALE_OF<S>::cv), c2 = (float)(1.0 / SCALE_OF<S>::cs);
+    // stations and PGV of the step, and the device step counter's advance
     CUDA_TRY(launch_station_pgv<S>(A_, g_.L, sta_xyz_, nsta_, d_.nt, step_, sta_wave_, pgv_, c1,
                                    c2, 1.0 / SCALE_OF<S>::cv, st));
-    CUDA_TRY(launch_step_advance(step_, st));
-    launches_ += 2;
+    launches_ += 1;
     ++it_;
     return CGFDM_OK;
   }
@@ -1022,7 +1022,7 @@ template <typename S> class EngineT : public Engine {
   int chunk_ = 0;             // planes per streaming work item in z; 0 = automatic
   bool chunk_fixed_ = false;  // set by set_chunk: the autotuner keeps chunk_
   bool drop_next_load_ = false;  // fault injection for failure-detection tests
-  int *step_ = nullptr;       // device copy of it_
+  int *step_ = nullptr;       // device copy of it_, then the end-of-step kernel's block counter
   float *moment_tab_ = nullptr;            // point-source moment per step
   int *fit_tab_ = nullptr;                 // fault interpolation index per step (-1: ended)
   float *ftw_tab_ = nullptr;               // fault interpolation weight per step

@@ -55,8 +55,8 @@ int encode_stream_maps(const S *wave, const S *cjm, const S *wm, const S *t, con
                        void *out);
 
 // Per-step values come from device memory so that a step can be replayed as
-// a CUDA graph: `step` points at the device step counter, advanced by
-// launch_step_advance at the end of every step.
+// a CUDA graph: `step` points at the device step counter, advanced by the
+// station / PGV launch at the end of every step.
 
 // Smoothed point source (singleSource.cpp:78-127) with the source moment
 // moment[*step]: adds value(cell) to Txx, Tyy, Tzz of w0 and, for cells in
@@ -76,14 +76,12 @@ cudaError_t launch_fault_source(S *w, long long fs, const long long *idx, const 
                                 const int *step, float DT, cudaStream_t st);
 
 // Station sampling (station.cpp:310-347) and PGV (PGV.cpp:49-101) of step
-// *step.
+// step[0], which the same launch then advances by one (step[1] is the
+// launch's block counter, zero between launches).
 template <typename S>
 cudaError_t launch_station_pgv(const S *w, Layout L, const int *xyz, int nsta, int NT,
-                               const int *step, float *wave, float *pgv, float c1, float c2,
+                               int *step, float *wave, float *pgv, float c1, float c2,
                                double cv_inv, cudaStream_t st);
-
-// ++*step (one thread).
-cudaError_t launch_step_advance(int *step, cudaStream_t st);
 
 // One field's interior slice at padded index `at` along axis 0/1/2, times
 // c (data_io.cpp:86-231).

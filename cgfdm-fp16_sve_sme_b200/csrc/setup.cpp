@@ -434,18 +434,27 @@ int build_fault(const std::string &dir, Setup &s, const Scale &sc) {
       }
     }
   }
-  // readSourceParams + solveMomentRate (multiSource.cpp:362-561)
+  // readSourceParams + solveMomentRate (multiSource.cpp:362-561): the
+  // records are read in order, then every (point, sample) is solved
+  // independently, in parallel
   const long long pn = (long long)point_index.size();
   std::vector<float> mr((size_t)pn * nt * 6, 0.0f);
-  long long row = 0;
-  for (auto &kv : point_index) {
-    f.seekg(12 + rec * kv.first + 3 * 4);
-    float asd[3];
-    f.read((char *)asd, sizeof asd);
-    std::vector<float> rake(nt), rate(nt);
-    f.read((char *)rake.data(), 4LL * nt);
-    f.read((char *)rate.data(), 4LL * nt);
-    if (!f) return fail(CGFDM_ERR_SOURCE, "source file is truncated");
+  std::vector<float> asd_all((size_t)pn * 3), rake_all((size_t)pn * nt), rate_all((size_t)pn * nt);
+  {
+    long long row = 0;
+    for (auto &kv : point_index) {
+      f.seekg(12 + rec * kv.first + 3 * 4);
+      f.read((char *)&asd_all[row * 3], 3 * sizeof(float));
+      f.read((char *)&rake_all[(size_t)row * nt], 4LL * nt);
+      f.read((char *)&rate_all[(size_t)row * nt], 4LL * nt);
+      if (!f) return fail(CGFDM_ERR_SOURCE, "source file is truncated");
+      ++row;
+    }
+  }
+  #pragma omp parallel for schedule(static)
+  for (long long row = 0; row < pn; ++row) {
+    const float *asd = &asd_all[row * 3];
+    const float *rake = &rake_all[(size_t)row * nt], *rate = &rate_all[(size_t)row * nt];
     float s_ = asd[1] * kDEG2RAD, d = asd[2] * kDEG2RAD, a = asd[0];
     for (int t = 0; t < nt; ++t) {
       float r = rake[t] * kDEG2RAD, rt = rate[t];
@@ -468,7 +477,6 @@ int build_fault(const std::string &dir, Setup &s, const Scale &sc) {
       m[4] = -M23 * a * rt;
       m[5] = -M13 * a * rt;
     }
-    ++row;
   }
   // dealDuplicateIndex (multiSource.cpp:566-624): the last row of a cell
   // accumulates the earlier rows of that cell in order.
@@ -495,6 +503,7 @@ int build_fault(const std::string &dir, Setup &s, const Scale &sc) {
         s.moment_rate[((size_t)J + (size_t)t * np) * 6 + q] = mr[((size_t)kv.second * nt + t) * 6 + q];
     ++J;
   }
+  #pragma omp parallel for schedule(static)
   for (int t = 0; t < nt; ++t)
     for (long long i = 0; i < np; ++i) {
       long long idx = s.src_index[i];

@@ -223,7 +223,7 @@ __device__ __forceinline__ unsigned slab_pos(const SlabDev<float> &sl, int i, in
 
 // PML auxiliary update of one slab point (pml_deriv.cpp:199-237,
 // pml_rk.cpp:15-69) given the direction's elastic combination E; adds
-// -beta * Aux * DT into h.  The auxiliaries are field-major on the device
+// -beta * Aux * DT into h (the point's slab corrections).  The auxiliaries are field-major on the device
 // (value v at v * np + pos), so the lanes of a warp, consecutive points of
 // the slab, touch consecutive addresses.
 //
@@ -625,6 +625,13 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
         const float bzd = bz_cur * DT * gz;
         float h[9], Lr[9], E[9];
         ElasticSum es;
+        // PML variant: the slab corrections -beta * Aux * DT of this point,
+        // added to the increment after the elastic sums
+        float pc[9];
+        if constexpr (PMLK) {
+#pragma unroll
+          for (int v = 0; v < 9; ++v) pc[v] = 0.0f;
+        }
         // Fields are taken in pairs (0,1) (2,3) (4,5) (6,7) and 8 for the
         // stencil sums, the increment and the RK combination.  The centre
         // tap of the x and y stencils, plane k at this point, is window slot
@@ -644,20 +651,12 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
           const XT *r0 = xy + (8 * BY + ys) * BX + xs;
           Lr[8] = stencil1(ldv(r0 - FB1), win[8][P1], ldv(r0 + FB1), ldv(r0 + 2 * FB1), ldv(r0 + 3 * FB1));
         }
+        es.add<true>(mx, bxd, Lr);
         if constexpr (PMLK) {
-          elastic9(mx, Lr, mu, lam, bu, E);
-#pragma unroll
-          for (int v = 0; v < 8; v += 2) {
-            const float2 hp = __fmul2_rn(pk(bxd), pk(E[v], E[v + 1]));
-            h[v] = hp.x;
-            h[v + 1] = hp.y;
-          }
-          h[8] = bxd * E[8];
           if (sx >= 0) {  // profile values d, alpha + d, beta at this x
-            pml_apply<RK>(a.slab[sx], slab_pos(a.slab[sx], i, j, k), E, dlx, adx, btx, DT, cB, cA, h, HP, pin);
+            elastic9(mx, Lr, mu, lam, bu, E);
+            pml_apply<RK>(a.slab[sx], slab_pos(a.slab[sx], i, j, k), E, dlx, adx, btx, DT, cB, cA, pc, HP, pin);
           }
-        } else {
-          es.add<true>(mx, bxd, Lr);
         }
         // y direction
 #pragma unroll
@@ -675,21 +674,13 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
           Lr[8] = stencil1(ldv(c0 - FB2 * BX), win[8][P1], ldv(c0 + FB2 * BX), ldv(c0 + 2 * FB2 * BX),
                            ldv(c0 + 3 * FB2 * BX));
         }
+        es.add<false>(my, byd, Lr);
         if constexpr (PMLK) {
-          elastic9(my, Lr, mu, lam, bu, E);
-#pragma unroll
-          for (int v = 0; v < 8; v += 2) {
-            const float2 hp = __ffma2_rn(pk(byd), pk(E[v], E[v + 1]), pk(h[v], h[v + 1]));
-            h[v] = hp.x;
-            h[v + 1] = hp.y;
-          }
-          h[8] += byd * E[8];
           if (sy >= 0) {
-            pml_apply<RK>(a.slab[sy], slab_pos(a.slab[sy], i, j, k), E, dly, ady, bty, DT, cB, cA, h,
+            elastic9(my, Lr, mu, lam, bu, E);
+            pml_apply<RK>(a.slab[sy], slab_pos(a.slab[sy], i, j, k), E, dly, ady, bty, DT, cB, cA, pc,
                           sh == sy ? HP : 0, pin);
           }
-        } else {
-          es.add<false>(my, byd, Lr);
         }
         // z direction: W[k - m*DIR] for m = -1..3 sits in slots P0 (q = k + DIR) .. P4
 #pragma unroll
@@ -701,23 +692,22 @@ __device__ __forceinline__ void stream_body(const Src &src, int *err) {
           Lr[v + 1] = s.y;
         }
         Lr[8] = stencil1(win[8][P0], win[8][P1], win[8][P2], win[8][P3], win[8][P4]);
+        es.add<false>(mz, bzd, Lr);
+        const bool zslab = PMLK && a.nslab && k < HALO + a.npml;
         if constexpr (PMLK) {
-          elastic9(mz, Lr, mu, lam, bu, E);
-#pragma unroll
-          for (int v = 0; v < 8; v += 2) {
-            const float2 hp = __ffma2_rn(pk(bzd), pk(E[v], E[v + 1]), pk(h[v], h[v + 1]));
-            h[v] = hp.x;
-            h[v + 1] = hp.y;
-          }
-          h[8] += bzd * E[8];
-          if (a.nslab && k < HALO + a.npml) {
+          if (zslab) {
+            elastic9(mz, Lr, mu, lam, bu, E);
             const float d = __ldg(pz + 2 * L.nz_ + k), btz = __ldg(pz + L.nz_ + k), adz = __ldg(pz + k) + d;
-            pml_apply<RK>(a.slab[2], slab_pos(a.slab[2], i, j, k), E, d * gz, adz, btz, DT, cB, cA, h,
+            pml_apply<RK>(a.slab[2], slab_pos(a.slab[2], i, j, k), E, d * gz, adz, btz, DT, cB, cA, pc,
                           sh == 2 ? HP : 0, pin);
           }
-        } else {
-          es.add<false>(mz, bzd, Lr);
-          es.finish(mu, lam, bu, h);
+        }
+        es.finish(mu, lam, bu, h);
+        if constexpr (PMLK) {
+          if (sx >= 0 || sy >= 0 || zslab) {
+#pragma unroll
+            for (int v = 0; v < 9; ++v) h[v] += pc[v];
+          }
         }
         // RK4 combination (wave_rk.cpp:13-99), two fields at a time:
         // stage 0: t = m + B1 h, out = m + A2 h (the stage input at k is the step state m);

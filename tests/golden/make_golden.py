@@ -21,7 +21,8 @@ run_point_fp16.npz
     on the finite-fault run (non-finite seismograms), so it has no fixture.
 c2_hill.npz, c3_201.npz
     The Gaussian-hill configuration (401 x 401 x 201, nPML 20, 121
-    stations, explosive source; 400 steps) and the 201 x 201 x 401
+    stations, explosive source; 400 steps; 8 x 1 ranks, so that no rank
+    boundary cuts the smoothed source) and the 201 x 201 x 401
     PerformanceTest shape (random terrain, layered medium, 80 x 40 finite
     fault; 700 steps, without the per-cell medium perturbation, which the
     reference's medium reader has no counterpart for) through the
@@ -277,7 +278,11 @@ def main():
     if "run_point_fp16" in want:
         run_fixture_fp16("run_point_fp16.npz", scenarios.run_point())
     if "c2_hill" in want:
-        bench_fixture("c2_hill.npz", scenarios.c2_parity(), 4, 2)
+        # 8 x 1 ranks: the smoothed point source (7^3 cells around i = 170,
+        # j = 200) must not straddle a rank boundary -- the reference adds it
+        # only inside the rank that holds its centre, so a split source would
+        # lose the part that falls into the halo
+        bench_fixture("c2_hill.npz", scenarios.c2_parity(), 8, 1)
     if "c3_201" in want:
         bench_fixture("c3_201.npz", scenarios.c3_201_parity(), 4, 2)
     print("golden fixtures written to", HERE)
