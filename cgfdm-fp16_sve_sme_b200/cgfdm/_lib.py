@@ -40,7 +40,7 @@ class Setup(C.Structure):
                 ("npts", C.c_int64), ("src_nt", C.c_int32), ("src_dt", C.c_float),
                 ("src_index", C.POINTER(C.c_int64)), ("moment_rate", C.POINTER(C.c_float)),
                 ("nsta", C.c_int32), ("sta_xyz", C.POINTER(C.c_int32)),
-                ("owner", C.c_void_p)]
+                ("owner", C.c_void_p), ("terrain", C.POINTER(C.c_float))]
 
 
 class StageBuffers(C.Structure):

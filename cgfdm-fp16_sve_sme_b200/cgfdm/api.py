@@ -377,6 +377,7 @@ def setup_from_directory(run_dir, precision=_lib.FP32):
         "moment_rate": f32(s.moment_rate, s.npts * s.src_nt * 6),
         "src_nt": s.src_nt, "src_dt": s.src_dt,
         "stations": _view(s.sta_xyz, 3 * s.nsta, C.c_int32, np.int32, owner).reshape(-1, 3),
+        "terrain": f32(s.terrain, nsurf).reshape(ny_, nx_),
         "precision": int(precision),
     }
 

@@ -291,3 +291,39 @@ def c3_workload(n, nsteps_total, perturbation=0.05, it_skip=10 ** 7, slice_free_
                 for a in range(11) for b in range(11)}
     return {"name": "c3-perftest-%dx%dx401" % (n, n), "params": p, "stations": stations,
             "terrain": terrain, "layers": layered_bytes(C2_LAYERS), "source": src}
+
+
+# --------------------------------------------------------------------------
+# SRTM90 DEM tiles (terrain.cpp:217-307): 6000 x 6000 float heights per 5 x 5
+# degree tile, x (longitude) fastest, file srtm_<lat>N<lon>E.bin
+# --------------------------------------------------------------------------
+DEM_POINTS = 6000
+
+
+def synthetic_dem_tile(lon0, lat0, seed, spikes=(), holes=()):
+    """A seeded smooth DEM tile (heights in metres, float32, shape (6000,
+    6000), row = latitude index): a few broad Gaussian mountains on a gentle
+    slope.  ``spikes`` (i, j, metres) add single-point peaks, the steep local
+    gradients the reader smooths away; ``holes`` (i, j) set the SRTM void
+    value -32768, which the reader resets to zero."""
+    rng = np.random.default_rng(seed)
+    ax = np.arange(DEM_POINTS, dtype=np.float64) / DEM_POINTS
+    X, Y = np.meshgrid(ax, ax)
+    h = 300.0 + 400.0 * X + 200.0 * Y
+    for _ in range(6):
+        cx, cy = rng.uniform(0.2, 0.8, 2)
+        w = rng.uniform(0.05, 0.3)
+        h += rng.uniform(500.0, 2500.0) * np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / w ** 2)
+    t = h.astype(np.float32)
+    for i, j, dz in spikes:
+        t[j, i] += np.float32(dz)
+    for i, j in holes:
+        t[j, i] = np.float32(-32768.0)
+    return t
+
+
+def write_dem_tile(dirpath, lon0, lat0, tile):
+    os.makedirs(dirpath, exist_ok=True)
+    fn = os.path.join(dirpath, "srtm_%dN%dE.bin" % (lat0, lon0))
+    np.ascontiguousarray(tile, np.float32).tofile(fn)
+    return fn

@@ -331,6 +331,7 @@ int cgfdm_setup_from_directory_ex(const char *run_dir, int32_t precision, cgfdm_
     out->moment_rate = s->moment_rate.data();
     out->nsta = (int32_t)s->sta_xyz.size() / 3;
     out->sta_xyz = s->sta_xyz.data();
+    out->terrain = s->terrain.data();
     out->owner = s.release();
     return CGFDM_OK;
   });

@@ -61,8 +61,216 @@ inline long long IDX(const Setup &s, int i, int j, int k) {
   return i + (long long)j * s.nx_ + (long long)k * s.nx_ * s.ny_;
 }
 
-// constructCoord (coord.cpp:106-402) with preprocessTerrain replaced by the
-// injected terrain of terrain_input.bin and the stretch of terrain.cpp:917-937.
+
+// ---------------------------------------------------------------------------
+// Real terrain from SRTM90 DEM tiles (terrain.cpp:217-940).
+//
+// The reference reads blockX x blockY tiles of 6000 x 6000 heights (5 degrees
+// each, srtm_<lat>N<lon>E.bin, x fastest), clears invalid elevations,
+// replaces the points of steep local gradient by their four-neighbour mean
+// and smooths with an 11 x 11 Gaussian inside the model's window, then
+// interpolates the DEM onto the grid (plus a 5-point margin) and smooths
+// again.  Grid points are mapped to longitude / latitude by PROJ's
+// azimuthal equidistant projection about (centerLongitude,
+// centerLatitude).  PROJ is not available to this library: the same
+// projection is evaluated on a sphere (radius kEarthRadius) with the inverse
+// formulas of Snyder (1987), eqs. 20-14 and 20-15.  Everything after the
+// projection keeps the reference's arithmetic and order.
+constexpr int kDemPointsPerBlock = 6000;  // terrain.cpp:15-16
+constexpr int kDemDegreesPerBlock = 5;    // terrain.cpp:12-13
+constexpr int kDemExpand = 10;            // callibrateTotalTerrain expandPoint
+constexpr double kEarthRadius = 6371008.8;
+constexpr double kRAD2DEG = 180.0 / (double)kPI;  // macro.h:62
+
+struct Aeqd {
+  double lam0, phi0, sin0, cos0;
+  Aeqd(double lon_0, double lat_0) {
+    // the centre passes through PROJ's "+lon_0=%lf +lat_0=%lf" string
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%lf %lf", lon_0, lat_0);
+    double lo = 0, la = 0;
+    std::sscanf(buf, "%lf %lf", &lo, &la);
+    const double d2r = M_PI / 180.0;
+    lam0 = lo * d2r;
+    phi0 = la * d2r;
+    sin0 = std::sin(phi0);
+    cos0 = std::cos(phi0);
+  }
+  // x, y in metres -> longitude, latitude in radians
+  void inverse(double x, double y, double &lam, double &phi) const {
+    const double rho = std::sqrt(x * x + y * y);
+    if (rho == 0.0) {
+      lam = lam0;
+      phi = phi0;
+      return;
+    }
+    const double c = rho / kEarthRadius, sc = std::sin(c), cc = std::cos(c);
+    phi = std::asin(cc * sin0 + y * sc * cos0 / rho);
+    lam = lam0 + std::atan2(x * sc, rho * cos0 * cc - y * sin0 * sc);
+  }
+};
+
+// GAUSS_FUN (macro.h:39) weights of the 11-point smoothing, nGauss = 5
+void dem_gauss(double Dg[11]) {
+  const int nGauss = 5;
+  const double ra = nGauss * 0.5;
+  for (int n = 0; n < 2 * nGauss + 1; ++n) {
+    const double t = (n - nGauss) - 0.0;
+    Dg[n] = std::exp(-((t / ra) * (t / ra))) / (ra * 1.772453850905516);
+  }
+}
+
+int build_srtm_terrain(const std::string &dir, Setup &s) {
+  const Params &p = s.p;
+  if (p.blockX <= 0 || p.blockY <= 0)
+    return fail(CGFDM_ERR_PARAMS, "SRTM90 needs blockX >= 1 and blockY >= 1");
+  const int totalX = (kDemPointsPerBlock - 1) * p.blockX + 1;
+  const int totalY = (kDemPointsPerBlock - 1) * p.blockY + 1;
+  const size_t ntot = (size_t)totalX * totalY;
+  std::vector<float> T(ntot, 0.0f);
+  // readSRTM90 (terrain.cpp:217-307): each tile's last row and column are
+  // dropped (shared with the next tile); the DEM's own last ones stay zero
+  {
+    std::vector<float> tile((size_t)kDemPointsPerBlock * kDemPointsPerBlock);
+    const std::string tdir = p.TerrainDir.empty() ? dir : (p.TerrainDir[0] == '/' ? p.TerrainDir
+                                                                                 : join(dir, p.TerrainDir));
+    for (int bj = 0; bj < p.blockY; ++bj)
+      for (int bi = 0; bi < p.blockX; ++bi) {
+        const int lat = p.latStart + kDemDegreesPerBlock * bj, lon = p.lonStart + kDemDegreesPerBlock * bi;
+        const std::string fn = tdir + "/srtm_" + std::to_string(lat) + "N" + std::to_string(lon) + "E.bin";
+        std::ifstream f(fn, std::ios::binary);
+        if (!f) return fail(CGFDM_ERR_IO, "missing DEM tile " + fn);
+        f.read((char *)tile.data(), sizeof(float) * tile.size());
+        if ((size_t)f.gcount() != sizeof(float) * tile.size())
+          return fail(CGFDM_ERR_IO, "DEM tile " + fn + " is shorter than 6000 x 6000 floats");
+        const int i0 = bi * (kDemPointsPerBlock - 1), j0 = bj * (kDemPointsPerBlock - 1);
+        #pragma omp parallel for schedule(static)
+        for (int jj = 0; jj < kDemPointsPerBlock - 1; ++jj)
+          for (int ii = 0; ii < kDemPointsPerBlock - 1; ++ii)
+            T[(size_t)(i0 + ii) + (size_t)(j0 + jj) * totalX] = tile[ii + (size_t)jj * kDemPointsPerBlock];
+      }
+  }
+  // resetTotalTerrain (terrain.cpp:309-325, ERROR_ELEVATION)
+  #pragma omp parallel for schedule(static)
+  for (long long q = 0; q < (long long)ntot; ++q)
+    if (T[q] < -32768 + 1.0 || T[q] > 32768 - 1.0) T[q] = 0.0f;
+
+  const float DH = (float)p.DH;
+  const Aeqd proj(p.centerLongitude, p.centerLatitude);
+  const double lonStart = p.lonStart, latStart = p.latStart;
+  const double deltaLon = double(kDemDegreesPerBlock * p.blockX) / double(totalX);
+  const double deltaLat = double(kDemDegreesPerBlock * p.blockY) / double(totalY);
+  double Dg[11];
+  dem_gauss(Dg);
+
+  // callibrateTotalTerrain (terrain.cpp:328-483): the window of DEM points
+  // around the grid's corners (calculateCutLonLatLoc, terrain.cpp:169-213)
+  {
+    const int I0 = 0, I1 = s.nx_, J0 = 0, J1 = s.ny_;  // frontN = 0 on a single rank
+    const double left = (I0 - H) * DH - p.centerX * DH, right = (I1 - H) * DH - p.centerX * DH;
+    const double down = (J0 - H) * DH - p.centerY * DH, up = (J1 - H) * DH - p.centerY * DH;
+    const double cx[4] = {left, left, right, right}, cy[4] = {down, up, down, up};
+    float maxLon = -1000.0, maxLat = -1000.0, minLon = 1000.0, minLat = 1000.0;
+    for (int c = 0; c < 4; ++c) {
+      double lam, phi;
+      proj.inverse(cx[c], cy[c], lam, phi);
+      const double Lon = lam * kRAD2DEG, Lat = phi * kRAD2DEG;
+      if (maxLon <= Lon) maxLon = Lon;
+      if (maxLat <= Lat) maxLat = Lat;
+      if (minLon >= Lon) minLon = Lon;
+      if (minLat >= Lat) minLat = Lat;
+    }
+    const int Is = int((minLon - lonStart) / deltaLon) - kDemExpand;
+    const int Js = int((minLat - latStart) / deltaLat) - kDemExpand;
+    const int Ie = int((maxLon - lonStart) / deltaLon) + kDemExpand;
+    const int Je = int((maxLat - latStart) / deltaLat) + kDemExpand;
+    if (Is - 6 < 0 || Js - 6 < 0 || Ie + 6 > totalX || Je + 6 > totalY)
+      return fail(CGFDM_ERR_PARAMS, "the model area reaches the edge of the DEM tiles");
+    std::vector<float> N(T);
+    #pragma omp parallel for schedule(static)
+    for (int j = Js; j < Je; ++j)
+      for (int i = Is; i < Ie; ++i) {
+        const size_t q = (size_t)i + (size_t)j * totalX;
+        const float a = T[q + 1], b = T[q - 1];
+        const float gx = a - b;
+        const float c = T[q + totalX], d = T[q - totalX];
+        const float gy = c - d;
+        const float grad = std::sqrt(gx * gx + gy * gy);
+        if (grad > 100.0) N[q] = (a + b + c + d) * 0.25;
+      }
+    T.swap(N);
+    N = T;
+    #pragma omp parallel for schedule(static)
+    for (int j = Js; j < Je; ++j)
+      for (int i = Is; i < Ie; ++i) {
+        double sum = 0.0;
+        for (int jj = j - 5; jj < j + 6; ++jj)
+          for (int ii = i - 5; ii < i + 6; ++ii) {
+            const double amp = Dg[ii + 5 - i] * Dg[jj + 5 - j] / 0.996768;
+            sum += amp * T[(size_t)ii + (size_t)jj * totalX];
+          }
+        N[(size_t)i + (size_t)j * totalX] = sum;
+      }
+    T.swap(N);
+  }
+
+  // terrainInterp (terrain.cpp:653-836) over the grid and a 5-point margin
+  const int nG = 5, enx = s.nx_ + 2 * nG, eny = s.ny_ + 2 * nG;
+  std::vector<float> ex((size_t)enx * eny);
+  int bad = 0;
+  #pragma omp parallel for schedule(static) reduction(+ : bad)
+  for (int j = 0; j < eny; ++j)
+    for (int i = 0; i < enx; ++i) {
+      const int I = i - nG, J = j - nG;  // frontN = 0
+      const double x = (I - H) * DH - p.centerX * DH, y = (J - H) * DH - p.centerY * DH;
+      double lam, phi;
+      proj.inverse(x, y, lam, phi);
+      const double x_ = lam * kRAD2DEG, y_ = phi * kRAD2DEG;
+      const int II = int((x_ - lonStart) / deltaLon), JJ = int((y_ - latStart) / deltaLat);
+      if (II < 0 || JJ < 0 || II + 1 >= totalX || JJ + 1 >= totalY) {
+        ++bad;
+        continue;
+      }
+      const double x1 = II * deltaLon + lonStart, y1 = JJ * deltaLat + latStart;
+      const double xs[2] = {x1, x1 + deltaLon}, ys[2] = {y1, y1 + deltaLat};
+      // the reference's corner order: z[1] and z[3] are both (I+1, J+1)
+      const double z[4] = {T[II + (size_t)JJ * totalX], T[II + 1 + (size_t)(JJ + 1) * totalX],
+                           T[II + 1 + (size_t)JJ * totalX], T[II + 1 + (size_t)(JJ + 1) * totalX]};
+      // interp2d (terrain.cpp:615-650)
+      double Lx[2], Ly[2];
+      for (int a = 0; a < 2; ++a) {
+        Lx[a] = 1;
+        for (int b = 0; b < 2; ++b)
+          if (a != b) Lx[a] = Lx[a] * (x_ - xs[b]) / (xs[a] - xs[b]);
+      }
+      for (int a = 0; a < 2; ++a) {
+        Ly[a] = 1;
+        for (int b = 0; b < 2; ++b)
+          if (a != b) Ly[a] = Ly[a] * (y_ - ys[b]) / (ys[a] - ys[b]);
+      }
+      double Li = 0.0;
+      for (int b = 0; b < 2; ++b)
+        for (int a = 0; a < 2; ++a) Li = Li + Lx[a] * Ly[b] * z[a * 2 + b];
+      ex[i + (size_t)j * enx] = Li;
+    }
+  if (bad) return fail(CGFDM_ERR_PARAMS, "grid points fall outside the DEM tiles");
+  #pragma omp parallel for schedule(static)
+  for (int j = nG; j < eny - nG; ++j)
+    for (int i = nG; i < enx - nG; ++i) {
+      double sum = 0;
+      for (int jj = j - nG; jj < j + nG + 1; ++jj)
+        for (int ii = i - nG; ii < i + nG + 1; ++ii) {
+          const double amp = Dg[ii + nG - i] * Dg[jj + nG - j] / 0.996768;
+          sum += amp * ex[ii + (size_t)jj * enx];
+        }
+      s.terrain[(i - nG) + (long long)(j - nG) * s.nx_] = sum;
+    }
+  return CGFDM_OK;
+}
+
+// constructCoord (coord.cpp:106-402): flat, Gaussian hill, the SRTM90 DEM
+// (preprocessTerrain, terrain.cpp:839-940) or a terrain injected as
+// terrain_input.bin, then the stretch of terrain.cpp:917-937.
 int build_coord(const std::string &dir, Setup &s) {
   const Params &p = s.p;
   const float DH = (float)p.DH;
@@ -104,15 +312,20 @@ int build_coord(const std::string &dir, Setup &s) {
         }
   }
   if (p.useTerrain) {
-    const int NXP = p.NX + 2 * H, NYP = p.NY + 2 * H;
-    std::ifstream f(join(dir, "terrain_input.bin"), std::ios::binary);
-    if (!f) return fail(CGFDM_ERR_IO, "useTerrain is set but terrain_input.bin is missing");
-    std::vector<float> g((size_t)NXP * NYP);
-    f.read((char *)g.data(), sizeof(float) * g.size());
-    if ((size_t)f.gcount() != sizeof(float) * g.size())
-      return fail(CGFDM_ERR_IO, "terrain_input.bin is shorter than (NX+6)*(NY+6) floats");
-    for (int j = 0; j < s.ny_; ++j)
-      for (int i = 0; i < s.nx_; ++i) s.terrain[i + (long long)j * s.nx_] = g[i + (size_t)j * NXP];
+    if (p.SRTM90 == 1) {
+      int rc = build_srtm_terrain(dir, s);
+      if (rc) return rc;
+    } else {
+      const int NXP = p.NX + 2 * H, NYP = p.NY + 2 * H;
+      std::ifstream f(join(dir, "terrain_input.bin"), std::ios::binary);
+      if (!f) return fail(CGFDM_ERR_IO, "useTerrain is set but terrain_input.bin is missing");
+      std::vector<float> g((size_t)NXP * NYP);
+      f.read((char *)g.data(), sizeof(float) * g.size());
+      if ((size_t)f.gcount() != sizeof(float) * g.size())
+        return fail(CGFDM_ERR_IO, "terrain_input.bin is shorter than (NX+6)*(NY+6) floats");
+      for (int j = 0; j < s.ny_; ++j)
+        for (int i = 0; i < s.nx_; ++i) s.terrain[i + (long long)j * s.nx_] = g[i + (size_t)j * NXP];
+    }
     double Depth = p.Depth * 1e3;
     #pragma omp parallel for schedule(static)
     for (int k = 0; k < s.nz_; ++k)
@@ -583,6 +796,9 @@ int load_params(const std::string &dir, Params &p) {
   I("sourceX", p.sourceX); I("sourceY", p.sourceY); I("sourceZ", p.sourceZ);
   S("sourceFile", p.sourceFile); S("sourceDir", p.sourceDir);
   F("mediumPerturbation", p.mediumPerturbation); I("mediumSeed", p.mediumSeed);
+  I("SRTM90", p.SRTM90); S("TerrainDir", p.TerrainDir);
+  I("lonStart", p.lonStart); I("latStart", p.latStart);
+  I("blockX", p.blockX); I("blockY", p.blockY);
   if (!p.useTerrain) p.Depth = p.DH * p.NZ * 1e-3;  // getParams.cpp:244-247
   return CGFDM_OK;
 }

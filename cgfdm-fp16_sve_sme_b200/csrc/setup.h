@@ -26,6 +26,9 @@ struct Params {
   int ShenModel = 0, Crust_1Medel = 0, LayeredModel = 0;
   std::string LayeredFileName, OUT, sourceFile, sourceDir;
   float Depth = 0;  // km
+  // real terrain from SRTM90 tiles (terrain.cpp:217-940)
+  int SRTM90 = 0, lonStart = 0, latStart = 0, blockX = 0, blockY = 0;
+  std::string TerrainDir;
   // Extensions of this implementation (absent from the reference):
   float mediumPerturbation = 0;  // +-fraction of a seeded uniform Vs/Vp perturbation
   int mediumSeed = 0;

@@ -402,6 +402,7 @@ typedef struct {
   int32_t nsta;
   int32_t *sta_xyz;       /* [nsta][3] padded */
   void *owner;            /* library-owned storage behind the arrays */
+  float *terrain;         /* [_ny_][_nx_] surface height before the stretch (m) */
 } cgfdm_setup;
 
 /* FP32 storage constants (cgfdm_setup_from_directory_ex with CGFDM_FP32). */

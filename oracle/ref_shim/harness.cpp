@@ -12,10 +12,13 @@
  *    (float32, (NY+6) rows of (NX+6) values, x fastest).  The rank's part is
  *    cut out and the reference's own vertical stretch is applied
  *    (terrain.cpp:917-937: z = -|Depth| + (h+|Depth|)/(NZ-1) * K).
+ *    The SRTM90 build (make ref-srtm, -DCGFDM_HARNESS_REF_TERRAIN) keeps the
+ *    reference's own preprocessTerrain instead.
  *  - readWeisenShenModel / readCrustal_1: not used by any fixture; they abort.
  */
 #include "header.h"
 
+#ifndef CGFDM_HARNESS_REF_TERRAIN
 void preprocessTerrain(PARAMS params, MPI_Comm comm_cart, MPI_COORD thisMPICoord, GRID grid,
                        float *coord, float *terrain) {
   (void)comm_cart;
@@ -55,6 +58,7 @@ void preprocessTerrain(PARAMS params, MPI_Comm comm_cart, MPI_COORD thisMPICoord
         coord[index + 2] = -abs(Depth) + DZ * K;
       }
 }
+#endif  // the SRTM90 build (make ref-srtm) compiles the reference's own terrain.cpp
 
 void readWeisenShenModel(PARAMS, GRID, MPI_COORD, float *, float *, float *) {
   printf("harness: the Shen crust model is not available\n");

@@ -30,6 +30,10 @@ c2_hill.npz, c3_201.npz
     the Vx/Vy/Vz seismograms of the stations, the PGV map and the last two
     free-surface snapshots.  A multi-rank reference run equals the
     single-rank one bit for bit (checked on run_fault.npz's inputs).
+srtm_run.npz
+    The SRTM90 terrain reader (terrain.cpp) on a seeded DEM tile: the
+    reference's own interpolated and smoothed terrain and a 30-step run on
+    it (see srtm_fixture).
 run_point.npz, run_fault.npz
     Complete reference runs (main.cpp -> run.cpp -> propagate.cpp) of small
     configurations: a flat half-space with the smoothed explosive point
@@ -248,7 +252,36 @@ def bench_fixture(name, sc, px, py, keep_snaps=2):
 
 
 FIXTURES = ["stage_small", "run_point", "run_fault", "c1_halfspace", "run_point_fp16",
-            "c2_hill", "c3_201"]
+            "c2_hill", "c3_201", "srtm_run"]
+
+
+def srtm_fixture():
+    """The SRTM90 terrain reader: scenarios.srtm_run through the reference's
+    FP32 build with its own terrain.cpp (make -C oracle ref-srtm; the map
+    projection is the spherical stand-in of oracle/ref_shim/proj.h), one
+    rank: the interior terrain it writes (terrain_mpi_0_0_0.bin) and the run's
+    seismograms, PGV and free-surface snapshots.  The 144 MB DEM tile is
+    regenerated from its seed by the tests."""
+    subprocess.check_call(["make", "-C", os.path.join(REPO, "oracle"), "ref-srtm", "-j8",
+                           "REF_ROOT=" + os.path.dirname(REF_SRC)], stdout=subprocess.DEVNULL)
+    exe = os.path.join(REF_DIR, "cgfdm_ref_fp32_srtm")
+    sc = scenarios.srtm_run()
+    work = tempfile.mkdtemp(prefix="cgfdm_golden_")
+    try:
+        scenarios.write_srtm_inputs(sc, work)
+        subprocess.check_call([exe], cwd=work, stdout=subprocess.DEVNULL)
+        outdir = os.path.join(work, sc["params"]["out"])
+        res = scenarios.read_outputs(sc, outdir)
+        p = sc["params"]
+        terrain = np.fromfile(os.path.join(outdir, "terrain_mpi_0_0_0.bin"), np.float32)
+        out = {"params_json": np.array(json.dumps(p)),
+               "stations_json": np.array(json.dumps(sc["stations"])),
+               "out_terrain": terrain.reshape(p["NY"], p["NX"])}
+        for k, v in res.items():
+            out["out_" + k] = v
+        np.savez_compressed(os.path.join(HERE, "srtm_run.npz"), **out)
+    finally:
+        shutil.rmtree(work)
 
 
 def main():
@@ -285,6 +318,8 @@ def main():
         bench_fixture("c2_hill.npz", scenarios.c2_parity(), 8, 1)
     if "c3_201" in want:
         bench_fixture("c3_201.npz", scenarios.c3_201_parity(), 4, 2)
+    if "srtm_run" in want:
+        srtm_fixture()
     print("golden fixtures written to", HERE)
 
 

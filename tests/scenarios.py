@@ -131,6 +131,34 @@ def c3_201_parity():
             "layers": as_u8(w["layers"]), "source": as_u8(w["source"])}
 
 
+def srtm_run():
+    """Real-terrain configuration through the SRTM90 reader: one 5 x 5 degree
+    DEM tile (100-105 E, 30-35 N, seeded, with steep spikes and void points
+    near the model), a 64 x 56 x 24 grid at 100 m centred on 102.5 E, 32.5 N,
+    two layers, an explosive point source, 30 steps.  The tile is 144 MB and
+    is written next to the run by write_srtm_inputs."""
+    p = S.params(NX=64, NY=56, NZ=24, nPML=6, DH=100.0, DT=0.008, TMAX=30 * 0.008 + 0.0001,
+                 **{"Depth(km)": 2.4}, centerX=32, centerY=28, useTerrain=1, useMedium=1,
+                 LayeredModel=1, SRTM90=1, TerrainDir="dem", lonStart=100, latStart=30,
+                 blockX=1, blockY=1, centerLongitude=102.5, centerLatitude=32.5,
+                 sourceX=32, sourceY=28, sourceZ=14, rickerfc=4.0, IT_SKIP=10, sliceFreeSurf=1,
+                 out="out")
+    stations = {"A": [10, 10, 23], "B": [32, 28, 23], "C": [50, 40, 23], "D": [20, 45, 12]}
+    return {"params": p, "stations": stations, "layers": as_u8(S.layered_bytes(TWO_LAYERS))}
+
+
+# the grid centre lies at DEM index (3000, 3000); spikes and voids within the
+# model's window (about +-50 points)
+SRTM_SPIKES = [(3010, 2995, 400.0), (2980, 3020, -350.0), (3025, 3012, 600.0)]
+SRTM_HOLES = [(2990, 2990), (3015, 2985)]
+
+
+def write_srtm_inputs(sc, dirpath):
+    write_inputs(sc, dirpath)
+    tile = S.synthetic_dem_tile(100, 30, seed=41, spikes=SRTM_SPIKES, holes=SRTM_HOLES)
+    S.write_dem_tile(os.path.join(dirpath, sc["params"]["TerrainDir"]), 100, 30, tile)
+
+
 def read_outputs(sc, outdir):
     """Reads the reference's single-rank outputs (station.cpp:382-405,
     PGV.cpp:103-111, data_io.cpp:323-495)."""
