@@ -293,10 +293,11 @@ def _setup_scenario(cgfdm, w, prec):
 
 
 def _sim_of(cgfdm, setup, prec, nt, device):
+    """A handle of one scenario; its tile form and work-item depth are the
+    autotuner's (alone), or its depth for the 32 x 16 form (in a batch)."""
     d0 = setup["desc"]
     sim = cgfdm.Simulation(cgfdm.make_desc(d0.nx, d0.ny, d0.nz, d0.npml, d0.dh, d0.dt, nt, prec,
                                            cgfdm.KERNEL_AUTO, device))
-    sim.set_tile_rows(16)
     sim.set_model(setup["cjm"], setup["rdz"])
     if setup["point"] is not None:
         sim.set_point_source(*setup["point"], setup["rickerfc"])
@@ -335,6 +336,10 @@ def bench_batch(args, cgfdm, torch, local, prec):
     batch = cgfdm.Batch(sims, graph=True)
     batch.run(args.warmup, stream.cuda_stream)
     torch.cuda.synchronize()
+    depths = {}
+    for sim in sims:
+        ch = sim.tuning()[1]
+        depths[str(ch)] = depths.get(str(ch), 0) + 1
     with ClockSampler(local) as clk:
         ev0.record(stream)
         batch.run(args.steps, stream.cuda_stream)
@@ -353,10 +358,12 @@ def bench_batch(args, cgfdm, torch, local, prec):
         "vs_baseline": None, "dtype": _dtype(args.precision), "data": "synthetic",
         "config": {"workload": "c4-batched-%d-scenarios" % n, "precision": args.precision,
                    "points_total": int(sum(pts)), "points_min": int(min(pts)),
-                   "points_max": int(max(pts)), "graph": True, "tile_rows": 16,
+                   "points_max": int(max(pts)), "graph": True, "tile_form": 16,
+                   "chunk_planes_histogram": depths,
                    "steps_note": "bounded sample of the 1500-step runs"},
         "serial": {"value": upd / (alone_ms / 1e3) / 1e9, "unit": UNIT,
-                   "note": "the same scenarios run alone back to back (no batch, no graph)"},
+                   "note": "the same scenarios run alone back to back (no batch, no graph; "
+                           "each with its own autotuned tile form and depth)"},
         "speedup_vs_serial": alone_ms / ms,
         "clocks": clk.summary(),
     }
@@ -483,7 +490,7 @@ def main():
     ap.add_argument("--cpu-baseline-steps", type=int, default=20)
     ap.add_argument("--batch-n", type=int, default=48, help="scenarios of --workload c4")
     ap.add_argument("--requests", type=int, default=32, help="requests of --workload c5")
-    ap.add_argument("--step-scale", type=float, default=0.1,
+    ap.add_argument("--step-scale", type=float, default=1.0,
                     help="--workload c5: request step counts are U[500, 3000] times this")
     ap.add_argument("--accuracy-workload", default="c2",
                     help="workload of the accuracy block (FP64 must fit one GPU)")

@@ -56,8 +56,8 @@ const int kFB[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1},  {-1, -1, 1},
 // nPML), shared by every handle of the process.
 std::mutex g_tune_mu;
 // autotuned (tile form, work-item depth) per (precision, nx, ny, nz, nPML,
-// fixed depth or -1)
-std::map<std::tuple<int, int, int, int, int, int>, std::pair<int, int>> g_tuned;
+// fixed depth or -1, batch member)
+std::map<std::tuple<int, int, int, int, int, int, int>, std::pair<int, int>> g_tuned;
 
 struct Dims {
   int nx, ny, nz, npml;
@@ -783,14 +783,16 @@ template <typename S> class EngineT : public Engine {
   // stage-1 auxiliary inputs; stage 1 reads those and writes Y and T; the
   // real step rewrites all of them before reading them, so the timing leaves
   // the run unchanged.  Results are cached per (precision, grid).
-  int tune(cudaStream_t st) {
+  // batch_form: a batch member, which always runs the 32 x 16 form inside
+  // its batch; only the depth is chosen and the member's own form is kept.
+  int tune(cudaStream_t st, bool batch_form = false) {
     const auto key = std::make_tuple((int)d_.precision, d_.nx, d_.ny, d_.nz, d_.npml,
-                                     chunk_fixed_ ? chunk_ : -1);
+                                     chunk_fixed_ ? chunk_ : -1, batch_form ? 1 : 0);
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
       auto f = g_tuned.find(key);
       if (f != g_tuned.end()) {
-        tile_rows_ = f->second.first;
+        if (!batch_form) tile_rows_ = f->second.first;
         chunk_ = f->second.second;
         return CGFDM_OK;
       }
@@ -802,6 +804,7 @@ template <typename S> class EngineT : public Engine {
     CUDA_TRY(cudaEventCreate(&e1));
     std::vector<int> forms = {16, 8};
     if (sizeof(S) == 2) forms.push_back(kTilePair);
+    if (batch_form) forms = {16};
     std::vector<int> chunks = {0, 64, 32};
     if (chunk_fixed_) chunks = {chunk_};
     int best_form = 16, best_chunk = chunks[0];
@@ -838,7 +841,7 @@ template <typename S> class EngineT : public Engine {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     CUDA_TRY(err);
-    tile_rows_ = best_form;
+    if (!batch_form) tile_rows_ = best_form;
     chunk_ = best_chunk;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tuned[key] = {best_form, best_chunk};
@@ -1098,6 +1101,15 @@ template <typename S> class BatchT : public BatchBase {
       CUDA_TRY(cudaStreamSynchronize(m->own_stream_));
       m->last_stream_ = st;
     }
+    if (!tuned_) {
+      // every member's work-item depth for the batch's 32 x 16 form
+      for (auto *m : m_)
+        if (m->use_stream_ && !m->chunk_fixed_) {
+          int rc = m->tune(st, true);
+          if (rc) return rc;
+        }
+      tuned_ = true;
+    }
     for (int s = 0; s < nsteps; ++s) {
       const int p = count_ % 8;
       if (use_graph_) {
@@ -1214,6 +1226,7 @@ template <typename S> class BatchT : public BatchBase {
   cudaGraphExec_t gexec_[8] = {};
   bool gseen_[8] = {};
   long long count_ = 0;  // steps run by this batch
+  bool tuned_ = false;   // members' work-item depths chosen (first run)
 };
 
 template <typename S>

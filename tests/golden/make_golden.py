@@ -32,7 +32,7 @@ c2_hill.npz, c3_201.npz
     single-rank one bit for bit (checked on run_fault.npz's inputs).
 srtm_run.npz
     The SRTM90 terrain reader (terrain.cpp) on a seeded DEM tile: the
-    reference's own interpolated and smoothed terrain and a 30-step run on
+    reference's own interpolated and smoothed terrain and a 120-step run on
     it (see srtm_fixture).
 run_point.npz, run_fault.npz
     Complete reference runs (main.cpp -> run.cpp -> propagate.cpp) of small

@@ -135,13 +135,14 @@ def srtm_run():
     """Real-terrain configuration through the SRTM90 reader: one 5 x 5 degree
     DEM tile (100-105 E, 30-35 N, seeded, with steep spikes and void points
     near the model), a 64 x 56 x 24 grid at 100 m centred on 102.5 E, 32.5 N,
-    two layers, an explosive point source, 30 steps.  The tile is 144 MB and
-    is written next to the run by write_srtm_inputs."""
-    p = S.params(NX=64, NY=56, NZ=24, nPML=6, DH=100.0, DT=0.008, TMAX=30 * 0.008 + 0.0001,
+    two layers, an explosive point source three cells below the surface, 120
+    steps (the wave crosses the surface stations).  The tile is 144 MB and is
+    written next to the run by write_srtm_inputs."""
+    p = S.params(NX=64, NY=56, NZ=24, nPML=6, DH=100.0, DT=0.008, TMAX=120 * 0.008 + 0.0001,
                  **{"Depth(km)": 2.4}, centerX=32, centerY=28, useTerrain=1, useMedium=1,
                  LayeredModel=1, SRTM90=1, TerrainDir="dem", lonStart=100, latStart=30,
                  blockX=1, blockY=1, centerLongitude=102.5, centerLatitude=32.5,
-                 sourceX=32, sourceY=28, sourceZ=14, rickerfc=4.0, IT_SKIP=10, sliceFreeSurf=1,
+                 sourceX=32, sourceY=28, sourceZ=20, rickerfc=4.0, IT_SKIP=40, sliceFreeSurf=1,
                  out="out")
     stations = {"A": [10, 10, 23], "B": [32, 28, 23], "C": [50, 40, 23], "D": [20, 45, 12]}
     return {"params": p, "stations": stations, "layers": as_u8(S.layered_bytes(TWO_LAYERS))}
