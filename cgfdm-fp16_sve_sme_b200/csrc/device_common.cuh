@@ -109,6 +109,9 @@ template <typename S> struct StageArgs {
   // planes per upper z chunk of the streaming kernel's work items (0: about
   // 40 items per CTA slot, chunks of at least 16 planes)
   int chunk;
+  // exact-order kernel only: points whose column lies in [skip_i0, skip_i1) x
+  // [skip_j0, skip_j1) are left to another kernel (empty box: none)
+  int skip_i0, skip_i1, skip_j0, skip_j1;
   // failure-detection tests only: the streaming kernel leaves one input-plane
   // load of its first work item unissued, so that the bounded wait on it
   // expires (no memory is touched); 0 in every normal launch

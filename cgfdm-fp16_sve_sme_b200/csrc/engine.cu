@@ -880,10 +880,7 @@ template <typename S> class EngineT : public Engine {
       // W out, plus m (stages 1, 2) and t (written in 0, updated in 1-2, read in 3)
       static const int nfield[4] = {39, 57, 57, 39};
       stream_bytes_ += (double)nfield[irk] * sizeof(S) * (double)(g_.nx) * g_.ny * (ksurf - HALO);
-      a.kbeg = ksurf;
-      a.kend = g_.L.nz_ - HALO;
-      CUDA_TRY(launch_stage_exact<S>(a, st));
-      ++launches_;
+      CUDA_TRY(launch_surface(a, st));
     } else {
       if (ev) {
         CUDA_TRY(cudaEventRecord(ev[1], st));
@@ -901,17 +898,30 @@ template <typename S> class EngineT : public Engine {
     return CGFDM_OK;
   }
 
-  // The exact-order kernel on the three free-surface layers of stage irk
-  // (the streaming part of the stage runs in a batch launch).
+  // The three free-surface layers of a fast-path stage: the tiled kernel on
+  // the columns outside the PML slabs, the exact-order kernel on the slab
+  // columns (FP64 runs the exact-order kernel only).
+  cudaError_t launch_surface(const StageArgs<S> &a0, cudaStream_t st) {
+    StageArgs<S> a = a0;
+    a.kbeg = g_.L.nz_ - HALO - 3;
+    a.kend = g_.L.nz_ - HALO;
+    if constexpr (std::is_same<S, double>::value) {
+      ++launches_;
+      return launch_stage_exact<S>(a, st);
+    } else {
+      launches_ += g_.npml > 0 ? 2 : 1;
+      return launch_stage_top<S>(a, st);
+    }
+  }
+
+  // The free-surface layers of stage irk (the streaming part of the stage
+  // runs in a batch launch).
   int launch_top(int irk, const int fb[3], cudaStream_t st) {
     static const int out_of[4] = {1, 2, 1, 0};
     StageArgs<S> a = stage_args(irk, fb);
     last_out_ = a.wout;
     last_aux_out_ = aux_total_ > 0 ? auxbuf(out_of[irk]) : nullptr;
-    a.kbeg = g_.L.nz_ - HALO - 3;
-    a.kend = g_.L.nz_ - HALO;
-    CUDA_TRY(launch_stage_exact<S>(a, st));
-    ++launches_;
+    CUDA_TRY(launch_surface(a, st));
     return CGFDM_OK;
   }
 

@@ -19,6 +19,11 @@ template <> struct SCALE_OF<__nv_bfloat16> { static constexpr double cv = 5.0e3,
 // Exact-order fused stage over the points kbeg <= k < kend (all i, j).
 template <typename S> cudaError_t launch_stage_exact(const StageArgs<S> &a, cudaStream_t st);
 
+// The three free-surface layers of the fast path: a shared-memory tiled
+// kernel for the columns outside every PML slab and the exact-order kernel
+// for the slab columns (FP32, FP16, BF16 storage).
+template <typename S> cudaError_t launch_stage_top(const StageArgs<S> &a, cudaStream_t st);
+
 // TMA-staged z-streaming fused stage over kbeg <= k < kend, which must lie
 // below the three free-surface layers.  `maps` holds the tensor maps of the
 // stage input wavefield and of the coefficients (encode_stream_maps).

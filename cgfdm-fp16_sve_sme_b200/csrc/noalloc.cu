@@ -165,7 +165,10 @@ int stage_noalloc(const cgfdm_stage_buffers &b, cudaStream_t st, unsigned char *
   }
   a.kbeg = ksurf;
   a.kend = L.nz_ - HALO;
-  NA_TRY(launch_stage_exact<S>(a, st));
+  if (overlap)
+    NA_TRY(launch_stage_exact<S>(a, st));
+  else  // the free-surface layers as a handle runs them
+    NA_TRY(launch_stage_top<S>(a, st));
   return CGFDM_OK;
 }
 

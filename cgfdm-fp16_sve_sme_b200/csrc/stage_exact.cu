@@ -87,6 +87,7 @@ __global__ void __launch_bounds__(256) stage_exact_kernel(StageArgs<S> a) {
   const int k = blockIdx.z * blockDim.z + threadIdx.z + a.kbeg;
   const int nx_ = a.L.nx_, ny_ = a.L.ny_, nz_ = a.L.nz_;
   if (i >= nx_ - HALO || j >= ny_ - HALO || k >= a.kend) return;
+  if (i >= a.skip_i0 && i < a.skip_i1 && j >= a.skip_j0 && j < a.skip_j1) return;
   const long long num = a.L.fs;  // field stride
   const long long sx = 1, sy = a.L.px, sz = a.L.plane;
   const long long c = a.L.at(i, j, k);
