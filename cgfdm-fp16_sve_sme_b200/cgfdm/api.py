@@ -137,9 +137,13 @@ class Simulation:
 
     def tuning(self):
         """(tile form, planes per work item) of the streaming kernel."""
-        v = np.zeros(2, np.int32)
+        return self.tuning3()[:2]
+
+    def tuning3(self):
+        """(tile form, planes per work item, tiled free-surface kernel 0/1)."""
+        v = np.zeros(3, np.int32)
         check(lib().cgfdm_get_tuning(self._h, _ptr(v)))
-        return int(v[0]), int(v[1])
+        return int(v[0]), int(v[1]), int(v[2])
 
     def set_tile_rows(self, rows):
         """Streaming-kernel tile height: 16, 8, or 0 to autotune at the first run."""

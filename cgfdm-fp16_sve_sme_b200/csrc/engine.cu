@@ -57,7 +57,11 @@ const int kFB[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1},  {-1, -1, 1},
 std::mutex g_tune_mu;
 // autotuned (tile form, work-item depth) per (precision, nx, ny, nz, nPML,
 // fixed depth or -1, batch member)
-std::map<std::tuple<int, int, int, int, int, int, int>, std::pair<int, int>> g_tuned;
+struct Tuned {
+  int form, chunk;
+  bool fast_top;  // free-surface layers on the tiled kernel (else the exact-order kernel)
+};
+std::map<std::tuple<int, int, int, int, int, int, int>, Tuned> g_tuned;
 
 struct Dims {
   int nx, ny, nz, npml;
@@ -709,6 +713,7 @@ template <typename S> class EngineT : public Engine {
   int get_tuning(int32_t *form_chunk) override {
     form_chunk[0] = use_stream_ ? (tile_rows_ ? tile_rows_ : 16) : 0;
     form_chunk[1] = use_stream_ ? chunk_ : 0;
+    form_chunk[2] = use_stream_ && fast_top_ ? 1 : 0;
     return CGFDM_OK;
   }
 
@@ -792,8 +797,11 @@ template <typename S> class EngineT : public Engine {
       std::lock_guard<std::mutex> lk(g_tune_mu);
       auto f = g_tuned.find(key);
       if (f != g_tuned.end()) {
-        if (!batch_form) tile_rows_ = f->second.first;
-        chunk_ = f->second.second;
+        if (!batch_form) {
+          tile_rows_ = f->second.form;
+          fast_top_ = f->second.fast_top;
+        }
+        chunk_ = f->second.chunk;
         return CGFDM_OK;
       }
     }
@@ -838,13 +846,34 @@ template <typename S> class EngineT : public Engine {
           best_chunk = ch;
         }
       }
+    // the free-surface layers: the tiled kernel (with the exact-order kernel
+    // on the PML-slab columns) against the exact-order kernel alone, on the
+    // surface of stage 0 (it writes X and T there, which stage 0 rewrites)
+    // (a batch member keeps its own choice, so that it computes the same
+    // bits alone and in the batch)
+    float surf_ms[2] = {0, 0};
+    for (int v = 0; v < 2 && err == cudaSuccess && !batch_form; ++v) {
+      fast_top_ = v == 0;
+      const StageArgs<S> s0 = stage_args(0, fb0);
+      const int l0 = launches_;
+      err = launch_surface(s0, st);
+      if (err == cudaSuccess) err = cudaEventRecord(e0, st);
+      for (int r = 0; r < 2 && err == cudaSuccess; ++r) err = launch_surface(s0, st);
+      if (err == cudaSuccess) err = cudaEventRecord(e1, st);
+      if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+      if (err == cudaSuccess) err = cudaEventElapsedTime(&surf_ms[v], e0, e1);
+      launches_ = l0;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     CUDA_TRY(err);
-    if (!batch_form) tile_rows_ = best_form;
+    if (!batch_form) {
+      fast_top_ = surf_ms[0] <= surf_ms[1];
+      tile_rows_ = best_form;
+    }
     chunk_ = best_chunk;
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tuned[key] = {best_form, best_chunk};
+    g_tuned[key] = {best_form, best_chunk, fast_top_};
     return CGFDM_OK;
   }
 
@@ -909,6 +938,10 @@ template <typename S> class EngineT : public Engine {
       ++launches_;
       return launch_stage_exact<S>(a, st);
     } else {
+      if (!fast_top_) {
+        ++launches_;
+        return launch_stage_exact<S>(a, st);
+      }
       launches_ += g_.npml > 0 ? 2 : 1;
       return launch_stage_top<S>(a, st);
     }
@@ -1034,6 +1067,7 @@ template <typename S> class EngineT : public Engine {
   int tile_rows_ = 0;         // streaming-kernel tile height; 0 = autotune at the first run()
   int chunk_ = 0;             // planes per streaming work item in z; 0 = automatic
   bool chunk_fixed_ = false;  // set by set_chunk: the autotuner keeps chunk_
+  bool fast_top_ = true;      // free-surface layers: tiled kernel + exact on slab columns
   bool drop_next_load_ = false;  // fault injection for failure-detection tests
   int *step_ = nullptr;       // device copy of it_, then the end-of-step kernel's block counter
   float *moment_tab_ = nullptr;            // point-source moment per step

@@ -192,10 +192,12 @@ int cgfdm_set_tile_rows(cgfdm_handle *h, int32_t rows);
  * L2) but re-read four planes per chunk. */
 int cgfdm_set_chunk(cgfdm_handle *h, int32_t planes);
 
-/* The streaming kernel's tile form and work-item depth in use (after the
- * autotuner, if it ran): form_chunk[0] = 16, 8 or 64, form_chunk[1] = planes
- * per item (0: automatic); both 0 when the handle runs the exact-order
- * kernel only. */
+/* The fast path's configuration in use (after the autotuner, if it ran),
+ * three values: form_chunk[0] = the streaming kernel's tile form 16, 8 or
+ * 64; form_chunk[1] = planes per work item (0: automatic); form_chunk[2] = 1
+ * if the free-surface layers run on the tiled kernel (the exact-order kernel
+ * on the PML-slab columns), 0 if on the exact-order kernel alone.  All 0 when
+ * the handle runs the exact-order kernel only. */
 int cgfdm_get_tuning(cgfdm_handle *h, int32_t *form_chunk);
 
 /* Checkpoint / resume at a step boundary (no counterpart in the reference):

@@ -157,17 +157,20 @@ def run_fixture_fp16(name, sc):
 
 def c1_fixture():
     """The half-space benchmark configuration (scenarios.c1, 1000 steps)
-    through the reference's FP32 build on one rank: seismograms, PGV and the
-    free-surface snapshots (inputs are regenerated from scenarios.c1; the
-    setup products are left out, the host setup is tested bit for bit
-    elsewhere)."""
+    through the reference's FP32 build on 8 x 1 MPI ranks (the point source
+    of the multi-source path is a single cell, so a rank split changes
+    nothing): seismograms, PGV and the free-surface snapshots every 333
+    steps (inputs are regenerated from scenarios.c1; the setup products are
+    left out, the host setup is tested bit for bit elsewhere)."""
     sc = scenarios.c1()
     exe = os.path.join(REF_DIR, "cgfdm_ref_fp32")
     work = tempfile.mkdtemp(prefix="cgfdm_golden_")
     try:
-        scenarios.write_inputs(sc, work)
-        subprocess.check_call([exe], cwd=work, stdout=subprocess.DEVNULL)
-        res = scenarios.read_outputs(sc, os.path.join(work, sc["params"]["out"]))
+        p = dict(sc["params"], PX=8, PY=1, PZ=1)
+        scenarios.write_inputs(dict(sc, params=p), work)
+        env = dict(os.environ, CGFDM_SHIM_NPROC="8", CGFDM_SHIM_TIMEOUT="7200")
+        subprocess.check_call([exe], cwd=work, env=env, stdout=subprocess.DEVNULL)
+        res = read_outputs_ranks(sc, os.path.join(work, p["out"]), 8, 1)
         out = {"params_json": np.array(json.dumps(sc["params"])),
                "stations_json": np.array(json.dumps(sc["stations"]))}
         for k, v in res.items():

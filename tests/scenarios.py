@@ -88,13 +88,13 @@ def c1():
     through the multi-source path, with the moment-rate time function of the
     reference's single source (singleSource.cpp:47-53: the derivative of a
     Ricker wavelet, f0 = 1.5 Hz) centred at t0 = 1.0 s; 25 surface stations
-    on a 5 x 5 lattice, 3 km apart; the free-surface snapshot at the last
-    step."""
+    on a 5 x 5 lattice, 3 km apart; free-surface snapshots every 333 steps
+    (mid-run while the wave crosses the surface, and the last step)."""
     nt = 1000
     dt = 0.008
     p = S.params(NX=161, NY=161, NZ=101, DH=100.0, DT=dt, TMAX=8.0001, nPML=12,
                  centerX=0, centerY=0, useMultiSource=1, **{"useSingleSource(ricker)": 0},
-                 IT_SKIP=999, sliceFreeSurf=1, out="out")
+                 IT_SKIP=333, sliceFreeSurf=1, out="out")
     f0, t0 = 1.5, 1.0
 
     def stf(t):

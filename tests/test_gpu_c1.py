@@ -4,8 +4,8 @@ path, 25 surface stations): the reference program on one GPU
 (cgfdm_run_directory) against the reference's own FP32 CPU build
 (tests/golden/c1_halfspace.npz).  The exact-order kernel reproduces every
 seismogram sample, the PGV map and the free-surface snapshots bit for bit;
-the streaming kernel stays within relative L2 1e-5 on the seismograms and
-the PGV map (the last snapshot: see below)."""
+the streaming kernel stays within relative L2 1e-5 on the seismograms, the
+PGV map and the mid-run free-surface snapshots."""
 import os
 import tempfile
 
@@ -54,10 +54,11 @@ def test_c1_streaming_kernel_within_1e5(c1_ref):
         err = rel_l2(got["station_wave"][:, :, v], c1_ref["out_station_wave"][:, :, v])
         assert err <= 1e-5, (v, err)
     assert rel_l2(got["pgv"], c1_ref["out_pgv"]) <= 1e-5
-    # the last snapshot (t = 8 s) holds only residual amplitudes of order
-    # 1e-10 -- the wave has left through the PML -- so its error is measured
-    # against the peak surface velocity of the run: RMS error / peak
-    snap, ref = got["freesurf"][-1], c1_ref["out_freesurf"][-1]
-    peak = np.abs(c1_ref["out_station_wave"][:, :, :3]).max()
-    rms = float(np.sqrt(np.mean((snap.astype(np.float64) - ref) ** 2)))
-    assert rms / peak <= 1e-5, rms / peak
+    # the free-surface snapshots at steps 333 and 666, while the wave crosses
+    # the surface: plain relative L2 (the last one, t = 8 s, holds only the
+    # residual left after the wave has gone out through the PML)
+    its = list(c1_ref["out_freesurf_its"])
+    for it in (333, 666):
+        q = its.index(it)
+        err = rel_l2(got["freesurf"][q], c1_ref["out_freesurf"][q])
+        assert err <= 1e-5, (it, err)
