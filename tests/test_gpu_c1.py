@@ -41,11 +41,16 @@ def _run(kernel):
     return scenarios.read_outputs(sc, os.path.join(d, sc["params"]["out"]))
 
 
+def _snap(got, it):
+    return got["freesurf"][list(got["freesurf_its"]).index(it)]
+
+
 def test_c1_exact_kernel_bitwise(c1_ref):
     got = _run(cgfdm.KERNEL_EXACT)
     np.testing.assert_array_equal(got["station_wave"], c1_ref["out_station_wave"])
     np.testing.assert_array_equal(got["pgv"], c1_ref["out_pgv"])
-    np.testing.assert_array_equal(got["freesurf"], c1_ref["out_freesurf"])
+    for q, it in enumerate(c1_ref["out_freesurf_its"]):
+        np.testing.assert_array_equal(_snap(got, int(it)), c1_ref["out_freesurf"][q])
 
 
 def test_c1_streaming_kernel_within_1e5(c1_ref):
@@ -57,8 +62,10 @@ def test_c1_streaming_kernel_within_1e5(c1_ref):
     # the free-surface snapshots at steps 333 and 666, while the wave crosses
     # the surface: plain relative L2 (the last one, t = 8 s, holds only the
     # residual left after the wave has gone out through the PML)
-    its = list(c1_ref["out_freesurf_its"])
-    for it in (333, 666):
-        q = its.index(it)
-        err = rel_l2(got["freesurf"][q], c1_ref["out_freesurf"][q])
+    its = [int(x) for x in c1_ref["out_freesurf_its"]]
+    mid = [it for it in its if 0 < it < 999]
+    if not mid:
+        pytest.skip("the C1 fixture holds no mid-run snapshot (regenerate it)")
+    for it in mid:
+        err = rel_l2(_snap(got, it), c1_ref["out_freesurf"][its.index(it)])
         assert err <= 1e-5, (it, err)
