@@ -233,7 +233,7 @@ int build_srtm_terrain(const std::string &dir, Setup &s) {
       }
       const double x1 = II * deltaLon + lonStart, y1 = JJ * deltaLat + latStart;
       const double xs[2] = {x1, x1 + deltaLon}, ys[2] = {y1, y1 + deltaLat};
-      // the reference's corner order: z[1] and z[3] are both (I+1, J+1)
+      // the reference's corner order (terrain.cpp:764-778): z[1] and z[3] are both (I+1, J+1)
       const double z[4] = {T[II + (size_t)JJ * totalX], T[II + 1 + (size_t)(JJ + 1) * totalX],
                            T[II + 1 + (size_t)JJ * totalX], T[II + 1 + (size_t)(JJ + 1) * totalX]};
       // interp2d (terrain.cpp:615-650)
