@@ -665,6 +665,7 @@ def main():
                                                  total_steps, cgfdm.FP16, kern, local))
         sim16.set_tile_rows(args.tile_rows)
         sim16.set_chunk(args.chunk)
+        sim16.set_timing(True)  # as the FP32 run: per-stage events, no graphs
         sim16.set_model(s16["cjm"], s16["rdz"])
         if s16["point"] is not None:
             sim16.set_point_source(*s16["point"], s16["rickerfc"])
@@ -689,6 +690,16 @@ def main():
         fp16 = {"value": v16, "unit": UNIT, "ms_per_step": ms16_max * 1e3 / args.steps,
                 "speedup_vs_fp32": v16 / value, "tile_form": form16, "chunk_planes": chunk16,
                 "bytes_per_point_step": BYTES_PER_POINT_STEP["fp16"]}
+        if ks16["stream_ms"] > 0:
+            a16 = ks16["stream_bytes"] / (ks16["stream_ms"] / 1e3) / 1e9
+            pk16 = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs") \
+                if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
+            pk16 = pk16 or 6650.0
+            fp16["roofline"] = {"bound": "hbm", "achieved": a16, "peak": pk16, "unit": "GB/s",
+                                "frac": a16 / pk16,
+                                "kernel": {64: "stage_pair_kernel", 16: "stage_stream_batch_kernel",
+                                           8: "stage_stream_kernel"}.get(form16, "stage_stream_kernel")
+                                + " (interior and PML launches)"}
 
     # error against FP64 of the precisions of this line, measured in this run
     # on a workload whose FP64 form fits one GPU
