@@ -448,6 +448,24 @@ def _dtype(p):
     return {"fp32": "f32", "fp64": "f64", "fp16": "f16-storage/f32", "bf16": "bf16-storage/f32"}[p]
 
 
+def measured_traffic(workload, kernel, precision, alg_bytes, launches):
+    """DRAM read + write bytes per launch (one stage's streaming launches) of
+    the kernel, from the one-pass ncu launch list of this workload, kernel and
+    precision (profiles/stage_traffic.json: DRAM bytes per algorithmic byte),
+    scaled to the algorithmic bytes of this run; None without a capture of
+    that exact combination."""
+    prof = os.path.join(ROOT, "profiles", "stage_traffic.json")
+    if not os.path.exists(prof) or launches <= 0:
+        return None
+    try:
+        for e in json.load(open(prof))["captures"]:
+            if (e["workload"], e["kernel"], e["precision"]) == (workload, kernel, precision):
+                return e["traffic_over_alg"] * alg_bytes / launches
+    except (OSError, ValueError, KeyError, TypeError):
+        return None
+    return None
+
+
 def replica_throughput(torch, dist, seconds, points, steps, world, device):
     """Whole-job throughput of N independent replicas (one per rank, the
     same work each): the slowest rank's time bounds the job, so the value is
@@ -695,11 +713,14 @@ def main():
             pk16 = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs") \
                 if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
             pk16 = pk16 or 6650.0
+            kn16 = {64: "stage_pair_kernel", 16: "stage_stream_batch_kernel",
+                    8: "stage_stream_kernel"}.get(form16, "stage_stream_kernel")
             fp16["roofline"] = {"bound": "hbm", "achieved": a16, "peak": pk16, "unit": "GB/s",
                                 "frac": a16 / pk16,
-                                "kernel": {64: "stage_pair_kernel", 16: "stage_stream_batch_kernel",
-                                           8: "stage_stream_kernel"}.get(form16, "stage_stream_kernel")
-                                + " (interior and PML launches)"}
+                                "traffic": measured_traffic(w["name"], kn16, "fp16",
+                                                            ks16["stream_bytes"],
+                                                            ks16["stream_launches"]),
+                                "kernel": kn16 + " (interior and PML launches)"}
 
     # error against FP64 of the precisions of this line, measured in this run
     # on a workload whose FP64 form fits one GPU
@@ -745,15 +766,7 @@ def main():
         slab_pts = 2 * npml * desc0.ny * kz + 2 * desc0.nx * npml * kz + desc0.nx * desc0.ny * npml
     aux_bytes = slab_pts * 144.0 * klaunch if kname != "stage_exact_kernel" else 0.0
     achieved_pml = (kbytes + aux_bytes) / (kms / 1e3) / 1e9 if kms > 0 else None
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "stage_traffic.json")
-    if os.path.exists(prof):
-        try:
-            t = json.load(open(prof)).get(kname, {}).get(args.precision)
-            if t:  # DRAM bytes of one ncu capture per algorithmic byte, scaled to this launch
-                traffic = t["traffic_over_alg"] * kbytes / max(klaunch, 1)
-        except Exception:  # noqa: BLE001
-            traffic = None
+    traffic = measured_traffic(w["name"], kname, args.precision, kbytes, klaunch)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

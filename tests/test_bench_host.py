@@ -61,3 +61,14 @@ def test_cpu_baseline_sample_of_large_grids():
     assert bench.cpu_sample_workload("c3-1201") == "c3-401"
     assert bench.cpu_sample_workload("c3-401") == "c3-401"
     assert bench.cpu_sample_workload("c2") == "c2"
+
+
+def test_traffic_figure_comes_only_from_a_capture_of_the_same_workload():
+    w = S.c2_workload(10)
+    t = bench.measured_traffic(w["name"], "stage_stream_kernel", "fp32", 4.0e9, 4)
+    assert t is not None and 1.0 < t / 1e9 < 2.0
+    # another kernel, precision or workload has no figure
+    assert bench.measured_traffic(w["name"], "stage_pair_kernel", "fp32", 4.0e9, 4) is None
+    assert bench.measured_traffic(w["name"], "stage_stream_kernel", "bf16", 4.0e9, 4) is None
+    assert bench.measured_traffic("c3-perftest-401x401x401", "stage_stream_kernel", "fp32",
+                                  4.0e9, 4) is None
