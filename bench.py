@@ -518,6 +518,8 @@ def main():
                          "seismograms and the free-surface snapshot against FP64 "
                          "(0: no accuracy block)"),
     args = ap.parse_args()
+    if args.e2e_steps < 1:
+        ap.error("--e2e-steps must be at least 1 (the line always carries an end-to-end figure)")
     if args.warmup < 3:
         args.warmup = 3
     ws, rank, local = dist_env()
@@ -702,11 +704,12 @@ def main():
         torch.cuda.synchronize()
         ms16 = ev0.elapsed_time(ev1)
         ks16 = sim16.kernel_stats()
-        form16, chunk16 = sim16.tuning()
+        form16, chunk16, top16 = sim16.tuning3()
         sim16.close()
         v16, ms16_max = replica_throughput(torch, dist, ms16 / 1e3, npts, args.steps, ws, "cuda")
         fp16 = {"value": v16, "unit": UNIT, "ms_per_step": ms16_max * 1e3 / args.steps,
                 "speedup_vs_fp32": v16 / value, "tile_form": form16, "chunk_planes": chunk16,
+                "surface_kernel": "tiled" if top16 else "exact-order",
                 "bytes_per_point_step": BYTES_PER_POINT_STEP["fp16"]}
         if ks16["stream_ms"] > 0:
             a16 = ks16["stream_bytes"] / (ks16["stream_ms"] / 1e3) / 1e9
