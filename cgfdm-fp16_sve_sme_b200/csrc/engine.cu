@@ -17,8 +17,11 @@
 // kernel everywhere (bit-identical to the reference's FP32 CPU build).
 #include <cuda_runtime.h>
 
+#include <unistd.h>
+
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -28,6 +31,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "json.h"
 #include "kernels.h"
 
 namespace cgfdm {
@@ -62,6 +66,83 @@ struct Tuned {
   bool fast_top;  // free-surface layers on the tiled kernel (else the exact-order kernel)
 };
 std::map<std::tuple<int, int, int, int, int, int, int>, Tuned> g_tuned;
+
+// Tuning choices kept across processes (optional).  When the environment
+// variable CGFDM_TUNE_CACHE names a file, a tuner that has no choice for its
+// key in this process looks it up there before timing anything, and every
+// choice it times is written back.  The file is a JSON object whose members
+// map a key naming the GPU (name and SM count), the precision, the grid, the
+// PML width, a fixed work-item depth (or -1) and batch membership to
+// [tile form, work-item depth, tiled free-surface kernel 0/1].  A malformed
+// file or entry is ignored (the tuner times as if it were absent); writers
+// replace the file whole through a rename, so concurrent processes can lose
+// each other's new entries but never leave a partial file.  The load and
+// the store are called with g_tune_mu held.
+std::string tune_cache_path() {
+  const char *p = std::getenv("CGFDM_TUNE_CACHE");
+  return p && *p ? std::string(p) : std::string();
+}
+std::string tune_cache_key(int device, const std::tuple<int, int, int, int, int, int, int> &k) {
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return std::string();
+  char buf[512];
+  std::snprintf(buf, sizeof buf, "%s|sm%d|precision%d|%dx%dx%d|npml%d|chunk%d|batch%d", prop.name,
+                prop.multiProcessorCount, std::get<0>(k), std::get<1>(k), std::get<2>(k),
+                std::get<3>(k), std::get<4>(k), std::get<5>(k), std::get<6>(k));
+  for (char *c = buf; *c; ++c)
+    if (*c == '"' || *c == '\\' || (unsigned char)*c < 0x20) *c = '_';
+  return buf;
+}
+bool tune_cache_load(const std::string &path, const std::string &key, int elem_bytes, Tuned &t) {
+  Json doc;
+  std::string err;
+  if (key.empty() || !Json::parse_file(path, doc, err) || doc.kind != Json::Object) return false;
+  for (const auto &m : doc.members) {
+    if (m.first != key) continue;
+    const Json &v = m.second;
+    if (v.kind != Json::Array || v.items.size() != 3) return false;
+    for (const Json &x : v.items)
+      if (x.kind != Json::Number) return false;
+    const int form = v.items[0].as_int(), chunk = v.items[1].as_int(), top = v.items[2].as_int();
+    const bool form_ok = form == 16 || form == 8 || (form == kTilePair && elem_bytes == 2);
+    if (!form_ok || chunk < 0 || (top != 0 && top != 1)) return false;
+    t = {form, chunk, top == 1};
+    return true;
+  }
+  return false;
+}
+void tune_cache_store(const std::string &path, const std::string &key, const Tuned &t) {
+  if (key.empty()) return;
+  std::vector<std::pair<std::string, std::string>> entries;  // key, serialised value
+  Json doc;
+  std::string err;
+  if (Json::parse_file(path, doc, err) && doc.kind == Json::Object) {
+    for (const auto &m : doc.members) {
+      const Json &v = m.second;
+      if (m.first == key || v.kind != Json::Array || v.items.size() != 3) continue;
+      char val[64];
+      std::snprintf(val, sizeof val, "[%d, %d, %d]", v.items[0].as_int(), v.items[1].as_int(),
+                    v.items[2].as_int());
+      std::string k = m.first;
+      for (char &c : k)
+        if (c == '"' || c == '\\' || (unsigned char)c < 0x20) c = '_';
+      entries.emplace_back(k, val);
+    }
+  }
+  char val[64];
+  std::snprintf(val, sizeof val, "[%d, %d, %d]", t.form, t.chunk, t.fast_top ? 1 : 0);
+  entries.emplace_back(key, val);
+  const std::string tmp = path + ".tmp." + std::to_string((long long)getpid());
+  FILE *f = std::fopen(tmp.c_str(), "w");
+  if (!f) return;
+  std::fprintf(f, "{\n");
+  for (size_t e = 0; e < entries.size(); ++e)
+    std::fprintf(f, "  \"%s\": %s%s\n", entries[e].first.c_str(), entries[e].second.c_str(),
+                 e + 1 < entries.size() ? "," : "");
+  std::fprintf(f, "}\n");
+  const bool ok = std::fclose(f) == 0;
+  if (!ok || std::rename(tmp.c_str(), path.c_str()) != 0) std::remove(tmp.c_str());
+}
 
 struct Dims {
   int nx, ny, nz, npml;
@@ -793,9 +874,15 @@ template <typename S> class EngineT : public Engine {
   int tune(cudaStream_t st, bool batch_form = false) {
     const auto key = std::make_tuple((int)d_.precision, d_.nx, d_.ny, d_.nz, d_.npml,
                                      chunk_fixed_ ? chunk_ : -1, batch_form ? 1 : 0);
+    const std::string cache = tune_cache_path();
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
       auto f = g_tuned.find(key);
+      if (f == g_tuned.end() && !cache.empty()) {
+        Tuned t;
+        if (tune_cache_load(cache, tune_cache_key(d_.device, key), (int)sizeof(S), t))
+          f = g_tuned.emplace(key, t).first;
+      }
       if (f != g_tuned.end()) {
         if (!batch_form) {
           tile_rows_ = f->second.form;
@@ -874,6 +961,7 @@ template <typename S> class EngineT : public Engine {
     chunk_ = best_chunk;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tuned[key] = {best_form, best_chunk, fast_top_};
+    if (!cache.empty()) tune_cache_store(cache, tune_cache_key(d_.device, key), g_tuned[key]);
     return CGFDM_OK;
   }
 

@@ -180,7 +180,11 @@ int cgfdm_get_kernel_stats(cgfdm_handle *h, double *out8);
  * elsewhere), or 0 (the default): autotune -- the first cgfdm_run times one
  * stage with each form on this handle's buffers (blocking that call for a
  * few stage times) and keeps the fastest; the choice is cached per
- * (precision, grid) for the process.  The forms split the grid differently
+ * (precision, grid) for the process.  If the environment variable
+ * CGFDM_TUNE_CACHE names a file, choices are also kept there across
+ * processes: a grid with an entry for this GPU is not timed again, and new
+ * choices are written back (a JSON object of [form, depth, tiled surface]
+ * triples; a malformed file is ignored and rewritten).  The forms split the grid differently
  * between the interior launch and the PML launch, whose variants round the
  * elastic combination differently, so they agree to rounding. */
 int cgfdm_set_tile_rows(cgfdm_handle *h, int32_t rows);
