@@ -18,6 +18,7 @@ compiled in place from the reference sources, run on all host cores as MPI
 ranks through the shared-memory MPI shim) on the same workload.
 """
 import argparse
+import contextlib
 import json
 import math
 import os
@@ -478,6 +479,42 @@ def replica_throughput(torch, dist, seconds, points, steps, world, device):
     return world * float(points) * steps / tmax / 1e9, tmax
 
 
+def setup_slots(params, local_ranks, avail):
+    """How many of a node's ranks may run the host setup at once: all of
+    them when the node's available memory holds their peak host footprint
+    (the 13 coefficient fields about 2.5 times over: the setup's own arrays,
+    the returned fields and their pinned copy), else as many as it holds
+    (at least one).  Ranks beyond that wait for a turn, so that N replicas
+    of a large grid do not drive the host out of memory."""
+    cjm_bytes = 13 * (params["NX"] + 6) * (params["NY"] + 6) * (params["NZ"] + 6) * 4
+    if not avail:
+        return local_ranks
+    return max(1, min(local_ranks, int(avail // (2.5 * cjm_bytes))))
+
+
+class SetupTurn:
+    """Holds one of `slots` node-wide setup slots (a file lock per slot under
+    the temporary directory; local rank r uses slot r mod slots) while a host
+    setup runs."""
+
+    def __init__(self, local, slots):
+        self.path = os.path.join(tempfile.gettempdir(),
+                                 "cgfdm_bench_setup.%s.%d.lock" % (
+                                     os.environ.get("MASTER_PORT", "0"), local % slots))
+        self.f = None
+
+    def __enter__(self):
+        import fcntl
+        self.f = open(self.path, "a")
+        fcntl.flock(self.f, fcntl.LOCK_EX)
+        return self
+
+    def __exit__(self, *a):
+        import fcntl
+        fcntl.flock(self.f, fcntl.LOCK_UN)
+        self.f.close()
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -564,10 +601,18 @@ def main():
 
     torch.cuda.set_device(local)
     dist = None
+    slots = 1
     if ws > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+        local_ranks = int(os.environ.get("LOCAL_WORLD_SIZE", str(ws)))
+        if args.workload not in ("c4", "c5"):
+            slots = setup_slots(make_workload(args.workload, 1)["params"], local_ranks,
+                                mem_available())
+        # ranks that wait for a setup turn reach the first barrier late: the
+        # timeout covers the waits (about a minute of setup per turn)
+        waits = (local_ranks + slots - 1) // slots - 1
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120 + 90 * waits),
                                 device_id=torch.device("cuda", local))
     prec = {"fp32": cgfdm.FP32, "fp16": cgfdm.FP16, "bf16": cgfdm.BF16, "fp64": cgfdm.FP64}[
         args.precision]
@@ -587,14 +632,33 @@ def main():
     w = make_workload(args.workload, max(total_steps, args.e2e_steps) + 2)
     d = tempfile.mkdtemp(prefix="cgfdm_bench_")
     write_workload(w, d)
+    def pinned(a):
+        t = torch.empty(a.shape, dtype={np.float32: torch.float32, np.int64: torch.int64}[
+            a.dtype.type], pin_memory=True)
+        t.numpy()[...] = a
+        return t.numpy()
+
     t0 = time.perf_counter()
-    # FP16 / BF16 handles take the coefficients in the reference's scaled form
-    setup = cgfdm.setup_from_directory(d, prec)
+    def setup_turn():
+        # a slot of the node's setup lock when its memory cannot hold every
+        # rank's setup at once (see setup_slots)
+        if slots < int(os.environ.get("LOCAL_WORLD_SIZE", "1")):
+            return SetupTurn(local, slots)
+        return contextlib.nullcontext()
+
+    with setup_turn():
+        # FP16 / BF16 handles take the coefficients in the reference's scaled form
+        setup = cgfdm.setup_from_directory(d, prec)
+        # the model coefficients (13 fields, 31 GB at 1201 x 1201 x 401 in
+        # FP32) are held once per rank, in pinned memory: the handles upload
+        # them from there, and the end-to-end run below takes them as its
+        # host input
+        cjm = pinned(setup["cjm"])
+        setup["cjm"] = None
     log("host setup %.1f s" % (time.perf_counter() - t0))
     shutil.rmtree(d, ignore_errors=True)
     desc0 = setup["desc"]
     npts = desc0.nx * desc0.ny * desc0.nz
-    cjm = setup["cjm"]
 
     def new_sim(nt):
         desc = cgfdm.make_desc(desc0.nx, desc0.ny, desc0.nz, desc0.npml, desc0.dh, desc0.dt, nt,
@@ -647,13 +711,7 @@ def main():
                            e2e_steps, prec, kern, local)
     sta = setup["stations"]
 
-    def pinned(a):
-        t = torch.empty(a.shape, dtype={np.float32: torch.float32, np.int64: torch.int64}[
-            a.dtype.type], pin_memory=True)
-        t.numpy()[...] = a
-        return t.numpy()
-
-    cjm_p, rdz_p = pinned(cjm), pinned(setup["rdz"])
+    cjm_p, rdz_p = cjm, pinned(setup["rdz"])
     has_fault = setup["src_index"].size > 0
     idx_p = pinned(setup["src_index"]) if has_fault else None
     rate_p = pinned(setup["moment_rate"]) if has_fault else None
@@ -668,6 +726,7 @@ def main():
     h2d = cjm.nbytes + setup["rdz"].nbytes + setup["moment_rate"].nbytes + \
         setup["src_index"].nbytes + sta.nbytes
     d2h = out_sta.nbytes + out_pgv.nbytes + out_fs.nbytes
+    del cjm  # the FP32 model's host copy is not needed past this point
 
     # the scaled-FP16 form on the same workload, timed the same way (the
     # metric pairs it with FP32; its error against FP64 comes from the
@@ -677,7 +736,8 @@ def main():
         d16 = tempfile.mkdtemp(prefix="cgfdm_bench_")
         try:
             write_workload(w, d16)
-            s16 = cgfdm.setup_from_directory(d16, cgfdm.FP16)
+            with setup_turn():
+                s16 = cgfdm.setup_from_directory(d16, cgfdm.FP16)
         finally:
             shutil.rmtree(d16, ignore_errors=True)
         e0 = s16["desc"]

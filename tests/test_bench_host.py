@@ -72,3 +72,41 @@ def test_traffic_figure_comes_only_from_a_capture_of_the_same_workload():
     assert bench.measured_traffic(w["name"], "stage_stream_kernel", "bf16", 4.0e9, 4) is None
     assert bench.measured_traffic("c3-perftest-401x401x401", "stage_stream_kernel", "fp32",
                                   4.0e9, 4) is None
+
+
+def test_setup_slots_follow_host_memory():
+    p = {"NX": 1201, "NY": 1201, "NZ": 401}
+    cjm = 13 * 1207 * 1207 * 407 * 4
+    assert bench.setup_slots(p, 8, None) == 8              # unknown: no limit
+    assert bench.setup_slots(p, 8, 100 * cjm) == 8         # room for all
+    assert bench.setup_slots(p, 8, 5 * cjm) == 2           # two at a time
+    assert bench.setup_slots(p, 8, 1 * cjm) == 1           # one at a time, never zero
+
+
+def test_setup_turns_of_one_slot_serialise(tmp_path, monkeypatch):
+    import multiprocessing as mp
+    import time
+
+    monkeypatch.setattr(bench.tempfile, "gettempdir", lambda: str(tmp_path))
+    monkeypatch.setenv("MASTER_PORT", "4711")
+    log = tmp_path / "log"
+    ctx = mp.get_context("fork")
+
+    def hold(local):
+        with bench.SetupTurn(local, 1):
+            with open(log, "a") as f:
+                f.write("in %d\n" % local)
+            time.sleep(0.3)
+            with open(log, "a") as f:
+                f.write("out %d\n" % local)
+
+    ps = [ctx.Process(target=hold, args=(r,)) for r in range(2)]
+    for q in ps:
+        q.start()
+    for q in ps:
+        q.join(30)
+        assert q.exitcode == 0
+    lines = log.read_text().split()
+    # the two holds do not interleave: in a, out a, in b, out b
+    assert lines[0::2] == ["in", "out", "in", "out"]
+    assert lines[1] == lines[3] and lines[5] == lines[7] and lines[1] != lines[5]
