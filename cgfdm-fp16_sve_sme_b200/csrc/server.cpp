@@ -15,7 +15,9 @@
 //     round each member's new seismogram rows are copied into the request's
 //     host buffer (streamed back chunk by chunk), finished requests copy
 //     their PGV map, release their device memory and leave the batch, and the
-//     requests admitted meanwhile join the next round.
+//     requests admitted meanwhile join the next round, after a short first
+//     round of their own (a tenth of the chunk, eager) that streams their
+//     first seismogram rows back early.
 // Wavefields stay resident on the device from admission to completion.
 // Latencies are measured from submission: to the first streamed seismogram
 // chunk, and to completion.
@@ -325,108 +327,133 @@ class Server {
     }
   }
 
+  using Slots = std::map<int, std::pair<std::vector<Engine *>, std::unique_ptr<BatchBase>>>;
+
   void loop() {
     cudaSetDevice(opts_.device);
     std::vector<Request *> active;
+    // a newly admitted request first advances this many steps in a round of
+    // its own (eager, no graphs), so that its first seismogram rows come back
+    // without waiting for a full round of every running request
+    const int first_chunk = std::max(1, opts_.chunk_steps / 10);
     for (;;) {
+      std::vector<Request *> fresh;
       {
         std::unique_lock<std::mutex> lk(mu_);
         work_cv_.wait(lk, [&] { return stopping_ || !ready_.empty() || !active.empty(); });
         if (stopping_) return;
         // requests admitted since the last round join this one
+        fresh = ready_;
         active.insert(active.end(), ready_.begin(), ready_.end());
         ready_.clear();
       }
       if (active.empty()) continue;
-      const auto t0 = Clock::now();
-      // one round: a batch per precision, each on its own stream
-      std::map<int, std::vector<Request *>> groups;
-      for (Request *r : active) groups[r->desc.precision].push_back(r);
-      std::vector<std::pair<std::vector<Request *>, int>> ran;
-      int q = 0;
-      for (auto &g : groups) {
-        std::vector<Request *> &m = g.second;
-        int k = opts_.chunk_steps;
-        for (Request *r : m) k = std::min(k, r->desc.nt - r->eng->steps_done());
-        std::vector<Engine *> e;
-        for (Request *r : m) e.push_back(r->eng.get());
-        BatchBase *b = batch_for(g.first, e);
-        int rc = b ? b->run(k, streams_[q++ % 4]) : CGFDM_ERR_ARG;
-        if (rc) {
-          batches_.erase(g.first);  // before the members' engines go
-          for (Request *r : m) r->eng.reset();
-          std::lock_guard<std::mutex> lk(mu_);
-          for (Request *r : m) {
-            active.erase(std::remove(active.begin(), active.end(), r), active.end());
-            fail(*r, rc);
+      if (!fresh.empty() && first_chunk < opts_.chunk_steps) {
+        run_round(active, fresh, first_chunk, fresh_batches_, false);
+        fresh_batches_.clear();  // one-off batches: their members join the main ones
+      }
+      if (!active.empty()) run_round(active, active, opts_.chunk_steps, batches_, opts_.use_graph);
+    }
+  }
+
+  // One round over `members` (a subset of `active`): a batch per precision,
+  // each on its own stream, advanced by at most `cap` steps; then the new
+  // seismogram rows are streamed back and finished requests retired (and
+  // removed from `active`).
+  void run_round(std::vector<Request *> &active, std::vector<Request *> members, int cap,
+             Slots &slots, bool graph) {
+    const auto t0 = Clock::now();
+    std::map<int, std::vector<Request *>> groups;
+    for (Request *r : members) groups[r->desc.precision].push_back(r);
+    std::vector<std::pair<std::vector<Request *>, int>> ran;
+    int q = 0;
+    for (auto &g : groups) {
+      std::vector<Request *> &m = g.second;
+      int k = cap;
+      for (Request *r : m) k = std::min(k, r->desc.nt - r->eng->steps_done());
+      std::vector<Engine *> e;
+      for (Request *r : m) e.push_back(r->eng.get());
+      BatchBase *b = batch_for(slots, g.first, e, graph);
+      int rc = b ? b->run(k, streams_[q++ % 4]) : CGFDM_ERR_ARG;
+      if (rc) {
+        // before the members' engines go
+        batches_.erase(g.first);
+        fresh_batches_.erase(g.first);
+        for (Request *r : m) r->eng.reset();
+        std::lock_guard<std::mutex> lk(mu_);
+        for (Request *r : m) {
+          active.erase(std::remove(active.begin(), active.end(), r), active.end());
+          fail(*r, rc);
+        }
+        done_cv_.notify_all();
+        cv_.notify_all();
+        continue;
+      }
+      ran.push_back({m, k});
+    }
+    // stream the new seismogram rows back; retire finished requests.  Order
+    // matters: results are copied first, then the batches that hold a
+    // finishing member are destroyed, then the members' engines, and only
+    // then is a request marked (wait() may release it at once).
+    struct Retire {
+      Request *r;
+      int rc;
+    };
+    std::vector<Retire> retire;
+    for (auto &g : ran) {
+      for (Request *r : g.first) {
+        const int it1 = r->eng->steps_done(), it0 = it1 - g.second;
+        int rc = r->eng->get_station_rows(r->wave.data(), it0, it1);
+        const bool finished = it1 >= r->desc.nt;
+        if (!rc && finished) rc = r->eng->get_pgv(r->pgv.data());
+        std::lock_guard<std::mutex> lk(mu_);
+        if (!rc) {
+          updates_ += (double)r->desc.nx * r->desc.ny * r->desc.nz * g.second;
+          if (r->steps == 0) {
+            r->t_first = Clock::now();
+            lat_first_.push_back(ms_between(r->t_submit, r->t_first));
           }
-          done_cv_.notify_all();
-          cv_.notify_all();
+          r->steps = it1;
+        }
+        if (rc || finished || r->cancel) retire.push_back({r, rc});
+      }
+    }
+    for (const Retire &x : retire) {
+      batches_.erase(x.r->desc.precision);
+      fresh_batches_.erase(x.r->desc.precision);
+    }
+    for (const Retire &x : retire) x.r->eng.reset();
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      for (const Retire &x : retire) {
+        Request *r = x.r;
+        active.erase(std::remove(active.begin(), active.end(), r), active.end());
+        if (x.rc) {
+          fail(*r, x.rc);
           continue;
         }
-        ran.push_back({m, k});
-      }
-      // stream the new seismogram rows back; retire finished requests.  Order
-      // matters: results are copied first, then the batches that hold a
-      // finishing member are destroyed, then the members' engines, and only
-      // then is a request marked (wait() may release it at once).
-      struct Retire {
-        Request *r;
-        int rc;
-      };
-      std::vector<Retire> retire;
-      for (auto &g : ran) {
-        for (Request *r : g.first) {
-          const int it1 = r->eng->steps_done(), it0 = it1 - g.second;
-          int rc = r->eng->get_station_rows(r->wave.data(), it0, it1);
-          const bool finished = it1 >= r->desc.nt;
-          if (!rc && finished) rc = r->eng->get_pgv(r->pgv.data());
-          std::lock_guard<std::mutex> lk(mu_);
-          if (!rc) {
-            updates_ += (double)r->desc.nx * r->desc.ny * r->desc.nz * g.second;
-            if (r->steps == 0) {
-              r->t_first = Clock::now();
-              lat_first_.push_back(ms_between(r->t_submit, r->t_first));
-            }
-            r->steps = it1;
-          }
-          if (rc || finished || r->cancel) retire.push_back({r, rc});
-        }
-      }
-      for (const Retire &x : retire) batches_.erase(x.r->desc.precision);
-      for (const Retire &x : retire) x.r->eng.reset();
-      {
-        std::lock_guard<std::mutex> lk(mu_);
-        for (const Retire &x : retire) {
-          Request *r = x.r;
-          active.erase(std::remove(active.begin(), active.end(), r), active.end());
-          if (x.rc) {
-            fail(*r, x.rc);
-            continue;
-          }
-          used_ -= r->bytes;
-          r->admitted = false;
-          if (r->cancel && r->steps < r->desc.nt) {
-            r->state = CGFDM_REQ_CANCELLED;
-            r->t_done = Clock::now();
-            continue;
-          }
+        used_ -= r->bytes;
+        r->admitted = false;
+        if (r->cancel && r->steps < r->desc.nt) {
+          r->state = CGFDM_REQ_CANCELLED;
           r->t_done = Clock::now();
-          t_last_done_ = r->t_done;
-          lat_done_.push_back(ms_between(r->t_submit, r->t_done));
-          r->state = CGFDM_REQ_DONE;
+          continue;
         }
-        busy_s_ += std::chrono::duration<double>(Clock::now() - t0).count();
+        r->t_done = Clock::now();
+        t_last_done_ = r->t_done;
+        lat_done_.push_back(ms_between(r->t_submit, r->t_done));
+        r->state = CGFDM_REQ_DONE;
       }
-      done_cv_.notify_all();
-      if (!retire.empty()) cv_.notify_all();  // memory came free
+      busy_s_ += std::chrono::duration<double>(Clock::now() - t0).count();
     }
+    done_cv_.notify_all();
+    if (!retire.empty()) cv_.notify_all();  // memory came free
   }
 
   // The batch of exactly these members (rebuilt when membership changes, so
   // that graphs are captured once per membership).
-  BatchBase *batch_for(int precision, const std::vector<Engine *> &m) {
-    auto &slot = batches_[precision];
+  BatchBase *batch_for(Slots &slots, int precision, const std::vector<Engine *> &m, bool graph) {
+    auto &slot = slots[precision];
     if (slot.first != m || !slot.second) {
       slot.second.reset();
       slot.first = m;
@@ -434,7 +461,7 @@ class Server {
         slot.second.reset();
         return nullptr;
       }
-      if (opts_.use_graph) slot.second->set_graph(true);
+      if (graph) slot.second->set_graph(true);
     }
     return slot.second.get();
   }
@@ -450,7 +477,8 @@ class Server {
   bool stopping_ = false;
   std::thread worker_, admitter_;
   cudaStream_t streams_[4] = {};
-  std::map<int, std::pair<std::vector<Engine *>, std::unique_ptr<BatchBase>>> batches_;
+  Slots batches_;        // the main batch of each precision (graphs, when on)
+  Slots fresh_batches_;  // the first, short round of newly admitted requests
   std::vector<double> lat_first_, lat_done_;
   double updates_ = 0, busy_s_ = 0;
   bool have_first_ = false;

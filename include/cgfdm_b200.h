@@ -263,7 +263,10 @@ int cgfdm_batch_destroy(cgfdm_batch *b);
  * (cgfdm_device_bytes) fits the HBM budget, keeps their wavefields resident,
  * and advances all admitted requests of one precision together as one batch
  * (cgfdm_batch) by chunk_steps steps per round -- the batches of different
- * precisions on their own streams, overlapping on the device.  After each
+ * precisions on their own streams, overlapping on the device.  A newly
+ * admitted request first runs chunk_steps / 10 steps (at least one) in a
+ * short round of the newcomers alone, so that its first seismogram rows come
+ * back without waiting for a full round of every running request.  After each
  * round the new seismogram rows of every request are copied back
  * (cgfdm_server_read_rows reads them while the request runs), finished
  * requests release their memory, and requests that arrived meanwhile join
